@@ -1,0 +1,306 @@
+"""Benchmark: exact negacyclic products per second at N=65536, L=1747 limbs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one product c = a*b mod (X^65536+1, q), q a 55904-bit random odd
+modulus (1747 limbs), a and b uniform in [0, q) (seeded synthetic inputs, 458 MB
+per operand: every step reads inputs larger than the 126 MB L2).
+
+  value     products/s, device-resident: operands already in HBM, K products
+            through negacyclic_run_device, CUDA events on the launching stream
+  e2e       products/s through negacyclic_run (the host-facing C ABI) with pinned
+            host buffers: H2D of a and b and D2H of c inside the timed region
+  roofline  the conversion GEMM (the largest kernel): algorithmic int8 ops per
+            launch / its CUDA-event time, against the int8 tensor peak
+  cpu_baseline  the GMP Kronecker oracle (the reference checker's algorithm) on a
+            bounded sample (N/32 coefficients, same q width), scaled to one product
+
+Multi-GPU (torchrun): one independent product stream per GPU (replicas, weak
+scaling), barrier + synchronize around the timed region, max time over ranks.
+--impl reference times the reference's CPU path (the oracle port, all host
+cores, one independent sample per core) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PACKAGE_DIR = os.path.join(REPO, "fherma-polynomial-cuda_b200")
+
+N, LIMBS, SEED = 65536, 1747, 2
+METRIC = "products/s at N=65536,W=1747 (limbs)"
+WORKLOAD = "negacyclic product N=65536, L=1747 limbs (55904-bit random odd q, seed 2), a,b uniform in [0,q)"
+CPU_SAMPLE_N = N // 32  # bounded CPU sample: 2048 coefficients of the same width
+
+
+def _load(name, path, package_dir=None):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path,
+                                                  submodule_search_locations=[package_dir] if package_dir else None)
+    module = importlib.util.module_from_spec(spec)
+    sys.modules[name] = module
+    spec.loader.exec_module(module)
+    return module
+
+
+def load_inputs():
+    return _load("fpc_b200_inputs", os.path.join(PACKAGE_DIR, "inputs.py"))
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+        return data["hbm_gbs"], data["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu: int):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={','.join(self.FIELDS)}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == len(self.FIELDS):
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(self.rows[0][2]) if self.rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_sample_seconds(sample_n: int, index: int = 0) -> float:
+    """One oracle product on the bounded sample (same q width, sample_n coefficients)."""
+    oracle = _load("negacyclic_oracle", os.path.join(REPO, "oracle", "oracle.py"))
+    inputs = load_inputs()
+    q, a, b = inputs.instance(sample_n, LIMBS, SEED, 1000 + index)
+    start = time.perf_counter()
+    oracle.kronecker(q, a, b)
+    return time.perf_counter() - start
+
+
+def _cpu_worker(args):
+    sample_n, index = args
+    return cpu_sample_seconds(sample_n, index)
+
+
+def distributed():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    """The reference's CPU path (GMP Kronecker, restated) on all host cores."""
+    world, rank, _ = distributed()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    scale = N // CPU_SAMPLE_N
+    with ctx.Pool(cores) as pool:
+        for w in range(args.warmup):
+            pool.map(_cpu_worker, [(CPU_SAMPLE_N, w * cores + i) for i in range(cores)])
+        start = time.perf_counter()
+        per_step = []
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(CPU_SAMPLE_N, 100 + k * cores + i) for i in range(cores)])
+            per_step.append(time.perf_counter() - t0)
+        total = time.perf_counter() - start
+    # each step: `cores` samples of 1/scale of a product each
+    value = args.steps * cores / scale / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mpz (GMP integers)",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sample": f"N={CPU_SAMPLE_N} of {N} coefficients"},
+        "cpu_baseline": {"value": value, "unit": "products/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} concurrent GMP Kronecker products of N={CPU_SAMPLE_N}, L={LIMBS} per step,"
+                                   f" scaled by {scale} to one N={N} product"},
+        "e2e": {"value": value, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = distributed()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    fpc = _load("fpc_b200", os.path.join(PACKAGE_DIR, "__init__.py"), PACKAGE_DIR)
+    inputs = load_inputs()
+    q, a, b = inputs.instance(N, LIMBS, SEED, rank)
+    plan = fpc.Plan(N, 32 * LIMBS, LIMBS, q, device=local)
+    info = plan.info()
+    stream = torch.cuda.Stream()
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.empty_like(da)
+    sptr = stream.cuda_stream
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- device-resident products
+    for _ in range(args.warmup):
+        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
+        stop.record(stream)
+        stop.synchronize()
+    device_ms = max_over_ranks(start.elapsed_time(stop))
+    barrier()
+    value = world * args.steps / (device_ms / 1000)
+
+    # --- per-stage CUDA-event times over the same number of products (roofline)
+    stage_ms = {name: 0.0 for name in fpc.STAGES}
+    for _ in range(args.steps):
+        for name, ms in plan.run_device_timed(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr).items():
+            stage_ms[name] += ms / args.steps
+
+    # --- end to end through the host-facing C ABI, pinned host buffers
+    pa = torch.from_numpy(a.view(np.int32)).pin_memory()
+    pb = torch.from_numpy(b.view(np.int32)).pin_memory()
+    pc = torch.empty_like(pa).pin_memory()
+    ha, hb, hc = (t.numpy().view(np.uint32) for t in (pa, pb, pc))
+    for _ in range(max(1, args.warmup)):
+        plan.run(ha, hb, out=hc)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plan.run(ha, hb, out=hc)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    e2e_value = world * args.steps / e2e_s
+    # the device product must equal the host-path product (both through the C ABI)
+    if not np.array_equal(dc.cpu().numpy().view(np.uint32), hc):
+        raise RuntimeError("device-resident and host products differ")
+
+    # --- roofline of the conversion GEMM: 2 ops per byte MAC, M=2N rows, K=4L bytes, 4r weight columns
+    hbm_gbs, bf16_tflops, source = peaks()
+    int8_peak = 2 * bf16_tflops  # dense int8 = 2x dense bf16 on B200
+    conv_ops = 2.0 * (2 * N) * (4 * LIMBS) * (4 * info["primes"])
+    crt_ops = 2.0 * N * (4 * info["primes"]) * (4 * info["words"])
+    conv_tops = conv_ops / (stage_ms["convert"] / 1000) / 1e12
+    roofline = {
+        "bound": "tensor", "kernel": "gemm_tc_kernel (conversion, tcgen05 kind::i8)",
+        "achieved": round(conv_tops, 1), "peak": round(int8_peak, 1), "unit": "TOPS (int8)",
+        "frac": round(conv_tops / int8_peak, 4), "traffic": None,
+        "peak_source": f"2 x bf16 dense of {source} ({bf16_tflops} TF/s)",
+        "algorithmic_ops_per_launch": conv_ops,
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "crt_gemm_tops": round(crt_ops / (stage_ms["crt"] / 1000) / 1e12, 1),
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        scale = N // CPU_SAMPLE_N
+        seconds = cpu_sample_seconds(CPU_SAMPLE_N)
+        cpu = {"value": 1.0 / (seconds * scale), "unit": "products/s", "cores": 1, "kind": "port",
+               "sample": f"one GMP Kronecker product (the reference checker's algorithm) of N={CPU_SAMPLE_N}, "
+                         f"L={LIMBS}, {seconds:.2f} s, scaled x{scale} to N={N}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "products/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": device_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (int8 tensor GEMMs, exact)", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "primes": info["primes"], "split": info["split"],
+                       "ntt_length": info["n_sub"], "tensor_gemms": info["gemm"],
+                       "l2": "inputs larger than L2 (458 MB per operand), no flush needed",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(a.nbytes + b.nbytes),
+                    "d2h_bytes_per_step": int(a.nbytes)},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": args.steps * info["kernels_per_product"],
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,386 @@
+// tcgen05 kind::i8 GEMM with TMA loads, an mbarrier pipeline and TMEM accumulators.
+//
+// Replaces the reference's sm_80 warp-MMA byte GEMM (tensor_product,
+// src/solve.cu:88-142: mma.sync m16n8k32 u8.u8.s32 with 64x16-word tiles) with
+// the Blackwell path: one CTA computes a 128 x 256 tile of D = A B^T
+// (A: [M][K] u8, B: [N][K] u8, both K-major), one thread issues
+// tcgen05.mma.cta_group::1.kind::i8 (M=128, N=256, K=32 bytes per instruction)
+// from 128B-swizzled shared-memory tiles that TMA fills through a 4-stage ring,
+// the s32 accumulator lives in 256 TMEM columns, and the epilogue reads it back
+// with tcgen05.ld and applies the conversion (REDC) or CRT (word sum) step.
+//
+// Exactness: each accumulator is a sum of K products of bytes, K * 255^2 < 2^31
+// for K <= 33024 (checked by the plan), so s32 accumulation is exact.
+//
+// Warp roles (128 threads, one warpgroup): warp 0 lane 0 = TMA producer,
+// warp 1 lane 0 = MMA issuer, warp 2 = TMEM allocator; all four warps run the
+// epilogue (warp w owns TMEM lanes / tile rows 32w..32w+31). Every mbarrier
+// wait is bounded (~2 s of SM clock); on timeout the kernel records an error
+// bit, still commits/waits what it issued, frees TMEM and returns.
+#include <cuda.h>
+
+#include <cstdio>
+
+#include "gemm_tc.cuh"
+
+namespace negacyclic {
+
+namespace {
+
+constexpr uint32_t kBlockM = 128, kBlockN = 256, kBlockK = 128;  // K in bytes (one 128B swizzle atom)
+constexpr uint32_t kStages = 4;
+constexpr uint32_t kATileBytes = kBlockM * kBlockK;                // 16 KB
+constexpr uint32_t kBTileBytes = kBlockN * kBlockK;                // 32 KB
+constexpr uint32_t kStageBytes = kATileBytes + kBTileBytes;
+constexpr uint32_t kTmemColumns = 256;
+constexpr uint32_t kGroupM = 16;                                   // m-tiles per raster group (L2 reuse of B)
+constexpr long long kTimeoutCycles = 4000000000ll;
+constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+
+__device__ uint32_t g_tc_error;
+
+// Instruction descriptor: D s32, A/B unsigned 8-bit, both K-major, M=128, N=256.
+constexpr uint32_t kInstrDesc = (2u << 4)              /* c_format = S32 */
+                                | (0u << 7) | (0u << 10) /* a/b format = u8 */
+                                | (0u << 15) | (0u << 16) /* K-major */
+                                | ((kBlockN >> 3) << 17) | ((kBlockM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(ptr));
+}
+
+// UMMA shared-memory descriptor for a K-major tile in the canonical 128B-swizzle
+// layout: rows of 128 bytes, 8-row core groups 1024 bytes apart (SBO), tile base
+// 1024-byte aligned (base offset 0), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_descriptor(uint32_t addr) {
+    uint64_t d = 0;
+    d |= uint64_t((addr & 0x3FFFFu) >> 4);
+    d |= uint64_t(1) << 16;           // leading byte offset (unused for swizzled K-major)
+    d |= uint64_t(1024 >> 4) << 32;   // stride byte offset
+    d |= uint64_t(1) << 46;           // version
+    d |= uint64_t(2) << 61;           // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    long long start = clock64();
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255u) == 255u && clock64() - start > kTimeoutCycles) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t desc_a, uint64_t desc_b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(desc_a), "l"(desc_b), "r"(kInstrDesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TileShape {
+    uint32_t m, columns, k_tiles, m_tiles, n_tiles;
+    RowMap rows;
+};
+
+__global__ void __launch_bounds__(128, 1) gemm_tc_kernel(const __grid_constant__ CUtensorMap a_map,
+                                                         const __grid_constant__ CUtensorMap b_map, TileShape shape,
+                                                         Epilogue epi) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* a_smem = smem;
+    uint8_t* b_smem = smem + kStages * kATileBytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(b_smem + kStages * kBTileBytes);
+    uint64_t* empty = full + kStages;
+    uint64_t* done = empty + kStages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+
+    // grouped raster: kGroupM m-tiles share each B tile while it is hot in L2
+    const uint32_t span = kGroupM * shape.n_tiles;
+    const uint32_t group = blockIdx.x / span, within = blockIdx.x - group * span;
+    const uint32_t first_m = group * kGroupM;
+    const uint32_t rows_in_group = min(kGroupM, shape.m_tiles - first_m);
+    const uint32_t m_tile = first_m + within % rows_in_group, n_tile = within / rows_in_group;
+    const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
+    // A-map coordinates of the tile's first row
+    uint32_t a_t = 0, a_row = row0;
+    if (shape.rows.mode == kRowsSplit) {
+        uint32_t op = row0 / shape.rows.n, rem = row0 - op * shape.rows.n;
+        a_t = rem / shape.rows.n_sub;
+        a_row = op * shape.rows.n_sub + (rem - a_t * shape.rows.n_sub);
+    }
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemColumns)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        uint32_t issued = 0;
+        for (uint32_t ks = 0; ks < shape.k_tiles; ++ks) {
+            const uint32_t s = ks % kStages, round = ks / kStages;
+            if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                ok = false;
+                break;
+            }
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_3d(a_smem + s * kATileBytes, &a_map, &full[s], int(ks * kBlockK), int(a_t), int(a_row));
+            tma_load_2d(b_smem + s * kBTileBytes, &b_map, &full[s], int(ks * kBlockK), int(col0));
+            issued = ks + 1;
+        }
+        if (!ok) {
+            // let the loads already issued land before the CTA can exit
+            for (uint32_t ks = (issued > kStages ? issued - kStages : 0); ks < issued; ++ks)
+                mbar_wait(&full[ks % kStages], (ks / kStages) & 1);
+            atomicOr(&g_tc_error, 1u);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        for (uint32_t ks = 0; ks < shape.k_tiles; ++ks) {
+            const uint32_t s = ks % kStages, round = ks / kStages;
+            if (!mbar_wait(&full[s], round & 1)) {
+                ok = false;
+                atomicOr(&g_tc_error, 2u);
+                break;
+            }
+            fence_after();
+            const uint32_t a_addr = smem_u32(a_smem + s * kATileBytes), b_addr = smem_u32(b_smem + s * kBTileBytes);
+#pragma unroll
+            for (uint32_t kk = 0; kk < kBlockK / 32; ++kk)
+                mma_i8(tmem, smem_descriptor(a_addr + kk * 32), smem_descriptor(b_addr + kk * 32),
+                       (ks | kk) != 0 ? 1u : 0u);
+            mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+        }
+        mma_commit(done);  // arrives when every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes)
+    const bool have = mbar_wait(done, 0);
+    if (!have && lane == 0) atomicOr(&g_tc_error, 4u);
+    fence_after();
+    const uint32_t row = row0 + warp * 32 + lane;
+    const bool row_ok = row < shape.m;
+    if (have) {
+        for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
+            const uint32_t c_base = col0 + chunk * 32;
+            if (c_base >= shape.columns) break;  // warp-uniform
+            uint32_t v[32];
+            tmem_load32(tmem + ((warp * 32) << 16) + chunk * 32, v);
+            if (!row_ok) continue;
+            if (epi.mode == kEpilogueRaw) {
+                int32_t* out = epi.raw + size_t(row) * epi.raw_ld;
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (c_base + j < shape.columns) out[c_base + j] = int32_t(v[j]);
+                continue;
+            }
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                const uint32_t group_index = c_base / 4 + g;
+                uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
+                             (uint64_t(v[4 * g + 3]) << 24);
+                if (epi.mode == kEpilogueConvert) {
+                    if (group_index < epi.r) {
+                        const DevicePrime f = epi.primes[group_index];
+                        uint32_t op = row / epi.n, rem = row - op * epi.n;
+                        epi.residues[(size_t(op) * epi.r + group_index) * epi.n + rem] = redc(s, f.p, f.pinv);
+                    }
+                } else if (group_index < epi.words) {
+                    epi.dots[size_t(row) * epi.words + group_index] = s;
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 2) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns)
+                     : "memory");
+    }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult status{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &status) == cudaSuccess &&
+            status == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(ptr);
+    }
+    return fn;
+}
+
+}  // namespace
+
+uint32_t* tensor_gemm_error_flag() {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_tc_error) != cudaSuccess) return nullptr;
+    return static_cast<uint32_t*>(ptr);
+}
+
+bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m,
+                         const uint8_t* b, uint32_t columns, uint32_t k_bytes, std::string& why) {
+    plan.ready = false;
+    EncodeTiled encode = encoder();
+    if (!encode) {
+        why = "cuTensorMapEncodeTiled unavailable";
+        return false;
+    }
+    if (k_bytes < kBlockK || k_bytes % 16 || a_pitch % 16 || a_pitch < k_bytes) {
+        why = "K must be >= 128 bytes with 16-byte rows";
+        return false;
+    }
+    if (reinterpret_cast<uintptr_t>(a) % 16 || reinterpret_cast<uintptr_t>(b) % 16) {
+        why = "operands must be 16-byte aligned";
+        return false;
+    }
+    if (columns < kBlockN) {
+        why = "fewer than 256 output columns";
+        return false;
+    }
+    uint32_t split = 1, slab = m;
+    if (rows.mode == kRowsSplit) {
+        split = rows.split;
+        slab = rows.n_sub;
+        if (m != 2 * rows.n) {
+            why = "split row map expects both operands";
+            return false;
+        }
+    }
+    if (slab < kBlockM || (rows.mode == kRowsSplit && slab % kBlockM)) {
+        why = "fewer than 128 rows per transform";
+        return false;
+    }
+    // A: dims (K bytes, s, rows/s); strides (pitch, s*pitch)
+    const cuuint64_t a_dims[3] = {k_bytes, split, uint64_t(m) / split};
+    const cuuint64_t a_strides[2] = {a_pitch, a_pitch * split};
+    const cuuint32_t a_box[3] = {kBlockK, 1, kBlockM};
+    const cuuint32_t unit[3] = {1, 1, 1};
+    CUresult ra = encode(&plan.a_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(a), a_dims, a_strides,
+                         a_box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const cuuint64_t b_dims[2] = {k_bytes, columns};
+    const cuuint64_t b_strides[1] = {k_bytes};
+    const cuuint32_t b_box[2] = {kBlockK, kBlockN};
+    CUresult rb = encode(&plan.b_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(b), b_dims, b_strides,
+                         b_box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (ra != CUDA_SUCCESS || rb != CUDA_SUCCESS) {
+        why = "tensor map encoding failed";
+        return false;
+    }
+    static bool attribute_set = false;
+    if (!attribute_set) {
+        if (cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            why = "cannot reserve shared memory";
+            return false;
+        }
+        attribute_set = true;
+    }
+    plan.m = m;
+    plan.columns = columns;
+    plan.k_bytes = k_bytes;
+    plan.m_tiles = (m + kBlockM - 1) / kBlockM;
+    plan.n_tiles = (columns + kBlockN - 1) / kBlockN;
+    plan.k_tiles = (k_bytes + kBlockK - 1) / kBlockK;
+    plan.rows = rows;
+    plan.error_flag = tensor_gemm_error_flag();
+    plan.ready = true;
+    return true;
+}
+
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {
+    TileShape shape{plan.m, plan.columns, plan.k_tiles, plan.m_tiles, plan.n_tiles, plan.rows};
+    gemm_tc_kernel<<<plan.m_tiles * plan.n_tiles, 128, kSmemBytes, stream>>>(plan.a_map, plan.b_map, shape,
+                                                                               epilogue);
+}
+
+}  // namespace negacyclic

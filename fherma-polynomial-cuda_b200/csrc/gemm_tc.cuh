@@ -1,0 +1,32 @@
+// Byte-sliced u8 x u8 -> s32 GEMM on the 5th-generation tensor cores (sm_100a).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "kernels.cuh"
+
+namespace negacyclic {
+
+struct TensorGemmPlan {
+    CUtensorMap a_map;   // 3-D view of A: (K bytes, s, rows / s), box (128, 1, 128), 128B swizzle
+    CUtensorMap b_map;   // 2-D view of B: (K bytes, columns),       box (128, 256),   128B swizzle
+    uint32_t m = 0, columns = 0, k_bytes = 0;
+    uint32_t m_tiles = 0, n_tiles = 0, k_tiles = 0;
+    RowMap rows{};
+    uint32_t* error_flag = nullptr;  // device word set when a pipeline wait times out
+    bool ready = false;
+};
+
+// Builds the tensor maps; false (with `why`) when the shape is outside what the
+// kernel handles (then the SIMT kernel is used).
+bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m,
+                         const uint8_t* b, uint32_t columns, uint32_t k_bytes, std::string& why);
+
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream);
+
+// Device word that records pipeline-wait timeouts of the tensor GEMM (0 = none).
+uint32_t* tensor_gemm_error_flag();
+
+}  // namespace negacyclic

@@ -1,0 +1,480 @@
+// SIMT stages of the negacyclic product and the parameter-only table builders.
+//
+// Data layout in HBM (one plan, r primes, ring split s, N' = N/s):
+//   operands   [2][N][Lp] u32      a then b, limbs padded to Lp = roundup(L, 4) (16-byte rows)
+//   residues   [2][r][N]  u32      per (operand, prime): s transforms of N' values,
+//                                  transform t holds coefficients i = s*j + t at j
+//   crt_in     [N][r']    u32      coefficient-major residues v_k (r' = roundup(r, 32))
+//   dots       [N][L+5]   u64      word sums of the byte-sliced CRT product
+//   twiddles   [r][N']    uint2    {w, floor(w 2^32/p)}: forward psi^brv(m), inverse psi^-brv(m),
+//                                  zeta psi^(2 brv(m)+1) (evaluation point at output m)
+#include "kernels.cuh"
+
+namespace negacyclic {
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+__global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                    uint32_t* __restrict__ out, uint32_t n, uint32_t limbs,
+                                    uint32_t padded) {
+    const uint64_t total = uint64_t(n) * padded;
+    for (uint64_t at = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; at < 2 * total;
+         at += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t within = at < total ? at : at - total;
+        const uint32_t* src = at < total ? a : b;
+        uint64_t row = within / padded;
+        uint32_t col = uint32_t(within - row * padded);
+        out[at] = col < limbs ? src[row * limbs + col] : 0u;
+    }
+}
+
+__device__ __forceinline__ uint32_t bit_reverse(uint32_t x, uint32_t bits) {
+    return bits ? (__brev(x) >> (32 - bits)) : 0u;
+}
+
+__global__ void twiddles_kernel(const DevicePrime* __restrict__ primes, uint32_t r, uint32_t n_sub,
+                                uint32_t log_n, uint2* fwd, uint2* inv, uint2* zeta) {
+    uint32_t k = blockIdx.y;
+    if (k >= r) return;
+    const DevicePrime f = primes[k];
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n_sub; m += gridDim.x * blockDim.x) {
+        uint32_t e = bit_reverse(m, log_n);
+        uint32_t w_fwd = pow_mod(f.psi, e, f);
+        uint32_t w_inv = pow_mod(f.psi, 2ull * n_sub - e, f);
+        uint32_t w_zeta = pow_mod(f.psi, 2ull * e + 1, f);
+        size_t at = size_t(k) * n_sub + m;
+        fwd[at] = make_uint2(w_fwd, shoup_quotient(w_fwd, f.p));
+        inv[at] = make_uint2(w_inv, shoup_quotient(w_inv, f.p));
+        zeta[at] = make_uint2(w_zeta, shoup_quotient(w_zeta, f.p));
+    }
+}
+
+// B_conv[4k+d][j] = byte_d(256^j mod p_k); zero for padded primes and j >= 4L.
+__global__ void convert_weights_kernel(const DevicePrime* __restrict__ primes, uint32_t r,
+                                       uint32_t padded_r, uint32_t limbs, uint32_t k_bytes,
+                                       uint8_t* out) {
+    uint32_t k = blockIdx.y;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < k_bytes; j += gridDim.x * blockDim.x) {
+        uint32_t w = 0;
+        if (k < r && j < 4 * limbs) w = pow_mod(256, j, primes[k]);
+        for (uint32_t d = 0; d < 4; ++d) out[(size_t(k) * 4 + d) * k_bytes + j] = uint8_t(w >> (8 * d));
+    }
+}
+
+// B_crt[c][4k+d] = byte_{c-d}(W_k), W_k given as `words` u32 words; zero outside.
+__global__ void crt_weights_kernel(const uint32_t* __restrict__ weights, uint32_t r, uint32_t padded_r,
+                                   uint32_t words, uint32_t columns, uint8_t* out) {
+    uint32_t c = blockIdx.y;
+    const uint32_t k_bytes = 4 * padded_r;
+    for (uint32_t kd = blockIdx.x * blockDim.x + threadIdx.x; kd < k_bytes; kd += gridDim.x * blockDim.x) {
+        uint32_t k = kd / 4, d = kd % 4;
+        uint8_t value = 0;
+        if (k < r && c < columns && c >= d) {
+            uint32_t at = c - d;  // byte position within W_k
+            if (at < 4 * words) value = uint8_t(weights[size_t(k) * words + at / 4] >> (8 * (at % 4)));
+        }
+        out[size_t(c) * k_bytes + kd] = value;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SIMT byte GEMM: D[m][c] = sum_j A[m][j] * B[c][j] with dp4a, 64x64 tiles,
+// 256 threads, each thread a 4-row x 4-column (one column group) micro-tile.
+constexpr int kTile = 64, kTileK = 64;
+
+__global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restrict__ a, uint64_t a_pitch,
+                                                        RowMap rows, uint32_t m_total,
+                                                        const uint8_t* __restrict__ b, uint32_t columns,
+                                                        uint32_t k_bytes, Epilogue epi) {
+    __shared__ uint32_t as[kTile][kTileK / 4 + 1];
+    __shared__ uint32_t bs[kTile][kTileK / 4 + 1];
+    const uint32_t tid = threadIdx.x, tr = tid / 16, tc = tid % 16;
+    const uint32_t m0 = blockIdx.x * kTile, c0 = blockIdx.y * kTile;
+    const uint32_t load_row = tid / 4, load_part = tid % 4;
+    const uint32_t am = m0 + load_row, bc = c0 + load_row;
+    const uint8_t* arow = am < m_total ? a + rows.row(am) * a_pitch : nullptr;
+    const uint8_t* brow = bc < columns ? b + size_t(bc) * k_bytes : nullptr;
+    uint32_t acc[4][4] = {};  // unsigned byte dot products (u8 x u8)
+    for (uint32_t k0 = 0; k0 < k_bytes; k0 += kTileK) {
+        uint32_t kk = k0 + load_part * 16;
+        uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
+        if (arow && kk < k_bytes) va = *reinterpret_cast<const uint4*>(arow + kk);
+        if (brow && kk < k_bytes) vb = *reinterpret_cast<const uint4*>(brow + kk);
+        as[load_row][load_part * 4 + 0] = va.x;
+        as[load_row][load_part * 4 + 1] = va.y;
+        as[load_row][load_part * 4 + 2] = va.z;
+        as[load_row][load_part * 4 + 3] = va.w;
+        bs[load_row][load_part * 4 + 0] = vb.x;
+        bs[load_row][load_part * 4 + 1] = vb.y;
+        bs[load_row][load_part * 4 + 2] = vb.z;
+        bs[load_row][load_part * 4 + 3] = vb.w;
+        __syncthreads();
+#pragma unroll
+        for (int kw = 0; kw < kTileK / 4; ++kw) {
+            uint32_t ra[4], rb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) ra[i] = as[tr * 4 + i][kw];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) rb[j] = bs[tc * 4 + j][kw];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = __dp4a(ra[i], rb[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    const uint32_t group = (c0 / 4) + tc;  // column group index (4 columns)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        uint32_t m = m0 + tr * 4 + i;
+        if (m >= m_total) continue;
+        if (epi.mode == kEpilogueRaw) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                uint32_t c = c0 + tc * 4 + j;
+                if (c < columns) epi.raw[size_t(m) * epi.raw_ld + c] = int32_t(acc[i][j]);
+            }
+            continue;
+        }
+        uint64_t s = uint64_t(uint32_t(acc[i][0])) + (uint64_t(uint32_t(acc[i][1])) << 8) +
+                     (uint64_t(uint32_t(acc[i][2])) << 16) + (uint64_t(uint32_t(acc[i][3])) << 24);
+        if (epi.mode == kEpilogueConvert) {
+            if (group >= epi.r) continue;
+            const DevicePrime f = epi.primes[group];
+            uint32_t op = m / epi.n, rem = m - op * epi.n;
+            epi.residues[(size_t(op) * epi.r + group) * epi.n + rem] = redc(s, f.p, f.pinv);
+        } else {
+            if (group < epi.words) epi.dots[size_t(m) * epi.words + group] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// NTT: one CTA per length-N' transform, whole transform in shared memory.
+
+__global__ void __launch_bounds__(512) ntt_forward_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
+                                                          const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
+                                                          uint32_t n_sub) {
+    extern __shared__ uint32_t x[];
+    const uint32_t t_index = blockIdx.x, k = blockIdx.y, op = blockIdx.z;
+    const uint32_t p = primes[k].p;
+    uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * n_sub;
+    const uint2* table = fwd + size_t(k) * n_sub;
+    for (uint32_t j = threadIdx.x; j < n_sub; j += blockDim.x) x[j] = data[j];
+    __syncthreads();
+    for (uint32_t m = 1, t = n_sub; m < n_sub; m *= 2) {
+        t /= 2;
+        for (uint32_t bfly = threadIdx.x; bfly < n_sub / 2; bfly += blockDim.x) {
+            uint32_t i = bfly / t, jj = bfly - i * t, j = 2 * i * t + jj;
+            uint2 w = table[m + i];
+            uint32_t u = x[j], v = shoup(x[j + t], w.x, w.y, p);
+            x[j] = add_mod(u, v, p);
+            x[j + t] = sub_mod(u, v, p);
+        }
+        __syncthreads();
+    }
+    for (uint32_t j = threadIdx.x; j < n_sub; j += blockDim.x) data[j] = x[j];
+}
+
+__global__ void __launch_bounds__(512) ntt_inverse_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
+                                                          const uint2* __restrict__ inv, uint32_t r, uint32_t n,
+                                                          uint32_t n_sub) {
+    extern __shared__ uint32_t x[];
+    const uint32_t v_index = blockIdx.x, k = blockIdx.y;
+    const DevicePrime f = primes[k];
+    uint32_t* data = residues + size_t(k) * n + size_t(v_index) * n_sub;
+    const uint2* table = inv + size_t(k) * n_sub;
+    for (uint32_t j = threadIdx.x; j < n_sub; j += blockDim.x) x[j] = data[j];
+    __syncthreads();
+    for (uint32_t m = n_sub, t = 1; m > 1; m /= 2, t *= 2) {
+        const uint32_t h = m / 2;
+        for (uint32_t bfly = threadIdx.x; bfly < n_sub / 2; bfly += blockDim.x) {
+            uint32_t i = bfly / t, jj = bfly - i * t, j = 2 * i * t + jj;
+            uint2 w = table[h + i];
+            uint32_t u = x[j], v = x[j + t];
+            x[j] = add_mod(u, v, f.p);
+            x[j + t] = shoup(sub_mod(u, v, f.p), w.x, w.y, f.p);
+        }
+        __syncthreads();
+    }
+    for (uint32_t j = threadIdx.x; j < n_sub; j += blockDim.x) data[j] = shoup(x[j], f.finish, f.finish_q, f.p);
+}
+
+// C_v = sum_{t+u=v} A_t B_u + zeta * sum_{t+u=v+s} A_t B_u at every evaluation point,
+// written over A_v. Products are Montgomery (x y 2^-32).
+template <int S>
+__global__ void pointwise_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
+                                 const uint2* __restrict__ zeta, uint32_t r, uint32_t n, uint32_t n_sub) {
+    const uint32_t k = blockIdx.y;
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_sub) return;
+    const DevicePrime f = primes[k];
+    uint32_t* a = residues + size_t(k) * n + m;
+    const uint32_t* b = residues + (size_t(r) + k) * n + m;
+    uint32_t av[S], bv[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+        av[t] = a[size_t(t) * n_sub];
+        bv[t] = b[size_t(t) * n_sub];
+    }
+    const uint2 z = zeta[size_t(k) * n_sub + m];
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        uint32_t low = 0, wrap = 0;
+#pragma unroll
+        for (int t = 0; t <= v; ++t) low = add_mod(low, mont(av[t], bv[v - t], f.p, f.pinv), f.p);
+#pragma unroll
+        for (int t = v + 1; t < S; ++t) wrap = add_mod(wrap, mont(av[t], bv[v + S - t], f.p, f.pinv), f.p);
+        a[size_t(v) * n_sub] = add_mod(low, shoup(wrap, z.x, z.y, f.p), f.p);
+    }
+}
+
+// residues[0][k][t*N'+j] -> crt_in[s*j+t][k]; zero for k in [r, r').
+__global__ void transpose_kernel(const uint32_t* __restrict__ residues, uint32_t* __restrict__ crt_in,
+                                 uint32_t r, uint32_t padded_r, uint32_t n, uint32_t n_sub, uint32_t split) {
+    __shared__ uint32_t tile[32][33];
+    const uint32_t rho0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const uint32_t x = threadIdx.x, y = threadIdx.y;
+    for (uint32_t dy = 0; dy < 32; dy += 8) {
+        uint32_t k = k0 + y + dy, rho = rho0 + x;
+        tile[y + dy][x] = (k < r && rho < n) ? residues[size_t(k) * n + rho] : 0u;
+    }
+    __syncthreads();
+    for (uint32_t dy = 0; dy < 32; dy += 8) {
+        uint32_t rho = rho0 + y + dy, k = k0 + x;
+        if (rho >= n || k >= padded_r) continue;
+        uint32_t t = rho / n_sub, j = rho - t * n_sub;
+        crt_in[(size_t(j) * split + t) * padded_r + k] = tile[x][y + dy];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-wide multiword arithmetic over 32-word chunks.
+
+// Carry into this lane given per-lane generate/propagate (mutually exclusive)
+// and the chain bit entering lane 0; updates `chain` to the carry out of lane 31.
+// Treats the 32 lanes as one 32-bit addition of (g|p) + g + chain.
+__device__ __forceinline__ uint32_t chain_carry(bool generate, bool propagate, uint32_t& chain) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t g = __ballot_sync(kFull, generate), gp = g | __ballot_sync(kFull, propagate);
+    uint64_t full = gp + g + chain;
+    uint32_t carries = uint32_t(full ^ gp ^ g);
+    chain = uint32_t(full >> 32);
+    return (carries >> lane) & 1u;
+}
+
+__device__ __forceinline__ uint32_t word_or_zero(const uint32_t* v, int64_t at, uint32_t size) {
+    return (at >= 0 && at < int64_t(size)) ? v[at] : 0u;
+}
+
+// bits [at, at+32) of the little-endian word array v (size words)
+__device__ __forceinline__ uint32_t bits_word(const uint32_t* v, int64_t at, uint32_t size) {
+    int64_t w = at >= 0 ? at / 32 : -((-at + 31) / 32);
+    uint32_t offset = uint32_t(at - w * 32);
+    uint64_t lo = word_or_zero(v, w, size), hi = word_or_zero(v, w + 1, size);
+    return uint32_t(((hi << 32) | lo) >> offset);
+}
+
+// v[0..len) += term(w) (term < 2^32), with carry; returns the final carry.
+template <class Term>
+__device__ __forceinline__ uint32_t add_words(uint32_t* v, uint32_t len, Term term) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t chain = 0;
+    for (uint32_t base = 0; base < len; base += 32) {
+        uint32_t w = base + lane;
+        uint32_t x = w < len ? v[w] : 0u, y = w < len ? term(w) : 0u;
+        uint64_t sum = uint64_t(x) + y;
+        uint32_t low = uint32_t(sum);
+        uint32_t carry = chain_carry((sum >> 32) != 0, low == kFull, chain);
+        if (w < len) v[w] = low + carry;
+    }
+    __syncwarp();
+    return chain;
+}
+
+// v[0..len) -= term(w), with borrow; returns the final borrow.
+template <class Term>
+__device__ __forceinline__ uint32_t sub_words(uint32_t* v, uint32_t len, Term term) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t chain = 0;
+    for (uint32_t base = 0; base < len; base += 32) {
+        uint32_t w = base + lane;
+        uint32_t x = w < len ? v[w] : 0u, y = w < len ? term(w) : 0u;
+        uint32_t borrow = chain_carry(x < y, x == y, chain);
+        if (w < len) v[w] = x - y - borrow;
+    }
+    __syncwarp();
+    return chain;
+}
+
+// sign of (v - q) over len words (q[w] = 0 for w >= limbs): -1, 0, 1
+__device__ __forceinline__ int compare_q(const uint32_t* v, uint32_t len, const uint32_t* q, uint32_t limbs) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (int64_t base = int64_t((len + 31) / 32 - 1) * 32; base >= 0; base -= 32) {
+        uint32_t w = uint32_t(base) + lane;
+        uint32_t x = w < len ? v[w] : 0u, y = w < limbs ? q[w] : 0u;
+        uint32_t differ = __ballot_sync(kFull, x != y);
+        if (differ) {
+            uint32_t top = 31 - __clz(differ);
+            int less = __shfl_sync(kFull, x < y ? 1 : 0, top);
+            return less ? -1 : 1;
+        }
+    }
+    return 0;
+}
+
+// One warp per coefficient; its words live in shared memory.
+__global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
+    extern __shared__ uint32_t scratch[];
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const uint32_t warps = blockDim.x / 32;
+    uint32_t* v = scratch + size_t(warp) * stride;
+    const uint32_t words = prm.words, limbs = prm.limbs, tlen = limbs + 2;
+    for (uint32_t i = blockIdx.x * warps + warp; i < prm.n; i += gridDim.x * warps) {
+        // 1. carry-save word sums -> exact words V (V < 2^(32 words))
+        const uint64_t* d = prm.dots + size_t(i) * words;
+        uint32_t chain = 0, carried_high = 0;
+        for (uint32_t base = 0; base <= words; base += 32) {
+            uint32_t w = base + lane;
+            uint64_t value = w < words ? d[w] : 0ull;
+            uint32_t high = uint32_t(value >> 32);
+            uint32_t below = __shfl_up_sync(kFull, high, 1);
+            if (lane == 0) below = carried_high;
+            carried_high = __shfl_sync(kFull, high, 31);
+            uint64_t sum = uint64_t(uint32_t(value)) + below;
+            uint32_t low = uint32_t(sum);
+            uint32_t carry = chain_carry((sum >> 32) != 0, low == kFull, chain);
+            if (w < stride) v[w] = low + carry;
+        }
+        __syncwarp();
+        // 2. CRT quotient K = (D + 2^63) >> 64, D = V >> 32(L+2)
+        const uint32_t kq = v[limbs + 4] + (v[limbs + 3] >> 31);
+        // 3. T' = T + K * (-P mod q), T = V mod 2^(32(L+2))
+        add_words(v, tlen, [&](uint32_t w) { return w < limbs ? uint32_t(uint64_t(kq) * prm.minus_p[w]) : 0u; });
+        add_words(v, tlen, [&](uint32_t w) {
+            return (w >= 1 && w - 1 < limbs) ? uint32_t((uint64_t(kq) * prm.minus_p[w - 1]) >> 32) : 0u;
+        });
+        // 4. Barrett quotient from the 128 bits of T' at q's top-64-bit window
+        uint64_t tl = uint64_t(bits_word(v, prm.top_shift, tlen)) |
+                      (uint64_t(bits_word(v, int64_t(prm.top_shift) + 32, tlen)) << 32);
+        uint64_t th = uint64_t(bits_word(v, int64_t(prm.top_shift) + 64, tlen)) |
+                      (uint64_t(bits_word(v, int64_t(prm.top_shift) + 96, tlen)) << 32);
+        uint64_t prod_l_hi = __umul64hi(tl, prm.mu_low);
+        uint64_t prod_h_lo = th * prm.mu_low, prod_h_hi = __umul64hi(th, prm.mu_low);
+        uint64_t word1 = prod_l_hi + prod_h_lo;
+        uint64_t word2 = prod_h_hi + (word1 < prod_l_hi ? 1 : 0);
+        uint64_t c2 = (tl + word1 < tl) ? 1 : 0;
+        const uint64_t quotient = th + word2 + c2;
+        const uint32_t ql = uint32_t(quotient), qh = uint32_t(quotient >> 32);
+        // 5. T' -= quotient * q, as four word streams
+        const uint32_t* q = prm.q;
+        sub_words(v, tlen, [&](uint32_t w) { return w < limbs ? uint32_t(uint64_t(ql) * q[w]) : 0u; });
+        sub_words(v, tlen, [&](uint32_t w) {
+            return (w >= 1 && w - 1 < limbs) ? uint32_t((uint64_t(ql) * q[w - 1]) >> 32) : 0u;
+        });
+        sub_words(v, tlen, [&](uint32_t w) {
+            return (w >= 1 && w - 1 < limbs) ? uint32_t(uint64_t(qh) * q[w - 1]) : 0u;
+        });
+        sub_words(v, tlen, [&](uint32_t w) {
+            return (w >= 2 && w - 2 < limbs) ? uint32_t((uint64_t(qh) * q[w - 2]) >> 32) : 0u;
+        });
+        // 6. at most three subtractions of q remain
+        int corrections = 0;
+        while (compare_q(v, tlen, q, limbs) >= 0) {
+            if (++corrections > 3) {
+                if (lane == 0) atomicOr(prm.error_flag, 1u);
+                break;
+            }
+            sub_words(v, tlen, [&](uint32_t w) { return w < limbs ? q[w] : 0u; });
+        }
+        // 7. canonical result
+        uint32_t* out = prm.out + size_t(i) * limbs;
+        for (uint32_t w = lane; w < limbs; w += 32) out[w] = v[w];
+        __syncwarp();
+    }
+}
+
+uint32_t log2_u32(uint32_t x) { return x ? 31 - __builtin_clz(x) : 0; }
+
+}  // namespace
+
+void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, uint32_t limbs,
+                         uint32_t padded_limbs, cudaStream_t stream) {
+    uint64_t total = 2ull * n * padded_limbs;
+    uint32_t blocks = uint32_t(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+    pad_operands_kernel<<<blocks, 256, 0, stream>>>(a, b, out, n, limbs, padded_limbs);
+}
+
+void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv, uint2* zeta,
+                     cudaStream_t stream) {
+    dim3 grid((n_sub + 255) / 256, r);
+    twiddles_kernel<<<grid, 256, 0, stream>>>(primes, r, n_sub, log2_u32(n_sub), fwd, inv, zeta);
+}
+
+void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,
+                            uint32_t k_bytes, uint8_t* out, cudaStream_t stream) {
+    dim3 grid((k_bytes + 255) / 256, padded_r);
+    convert_weights_kernel<<<grid, 256, 0, stream>>>(primes, r, padded_r, limbs, k_bytes, out);
+}
+
+void launch_crt_weights(const uint32_t* weights_words, uint32_t r, uint32_t padded_r, uint32_t words,
+                        uint32_t columns, uint8_t* out, cudaStream_t stream) {
+    dim3 grid((4 * padded_r + 255) / 256, columns);
+    crt_weights_kernel<<<grid, 256, 0, stream>>>(weights_words, r, padded_r, words, columns, out);
+}
+
+void launch_gemm_simt(const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m, const uint8_t* b,
+                      uint32_t columns, uint32_t k_bytes, const Epilogue& epilogue, cudaStream_t stream) {
+    dim3 grid((m + kTile - 1) / kTile, (columns + kTile - 1) / kTile);
+    gemm_simt_kernel<<<grid, 256, 0, stream>>>(a, a_pitch, rows, m, b, columns, k_bytes, epilogue);
+}
+
+static uint32_t ntt_threads(uint32_t n_sub) {
+    uint32_t half = n_sub / 2;
+    return half >= 512 ? 512 : (half >= 32 ? half : 32);
+}
+
+void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r, uint32_t n,
+                        uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    dim3 grid(split, r, 2);
+    ntt_forward_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, fwd, r, n,
+                                                                                          n_sub);
+}
+
+void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r, uint32_t n,
+                        uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    dim3 grid(split, r);
+    ntt_inverse_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, inv, r, n,
+                                                                                          n_sub);
+}
+
+void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r, uint32_t n,
+                      uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    dim3 grid((n_sub + 127) / 128, r);
+    switch (split) {
+        case 1: pointwise_kernel<1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 2: pointwise_kernel<2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 4: pointwise_kernel<4><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 8: pointwise_kernel<8><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        default: pointwise_kernel<16><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+    }
+}
+
+void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r, uint32_t n,
+                      uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    dim3 grid((n + 31) / 32, padded_r / 32);
+    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, n_sub, split);
+}
+
+void launch_reduce(const ReduceParams& params, cudaStream_t stream) {
+    const uint32_t warps = 8;
+    const uint32_t stride = (params.words + 1 + 31) / 32 * 32;
+    const size_t smem = size_t(warps) * stride * sizeof(uint32_t);
+    uint32_t blocks = (params.n + warps - 1) / warps;
+    if (blocks > 148u * 8) blocks = 148u * 8;
+    reduce_kernel<<<blocks, warps * 32, smem, stream>>>(params, stride);
+}
+
+}  // namespace negacyclic

@@ -1,0 +1,76 @@
+// Device kernels of the negacyclic product (SIMT stages and table builders).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "modarith.cuh"
+
+namespace negacyclic {
+
+// Row addressing of the u8 GEMM's A operand.
+//  kRowsLinear:   row m at base + m * pitch
+//  kRowsSplit:    row rho = op*N + t*N' + j reads coefficient i = s*j + t of operand op
+//                 from base + (op*N + i) * pitch  (conversion of the split ring)
+enum RowMode : int { kRowsLinear = 0, kRowsSplit = 1 };
+
+struct RowMap {
+    int mode;
+    uint32_t n, n_sub, split;
+    __device__ __forceinline__ uint64_t row(uint32_t m) const {
+        if (mode == kRowsLinear) return m;
+        uint32_t op = m / n, rem = m - op * n;
+        uint32_t t = rem / n_sub, j = rem - t * n_sub;
+        return uint64_t(op) * n + uint64_t(j) * split + t;
+    }
+};
+
+// Epilogues of the byte-sliced GEMM. Output column group g (4 consecutive
+// columns 4g..4g+3) of row m holds int32 dots G_d; S = sum_d G_d 256^d.
+enum EpilogueMode : int { kEpilogueRaw = 0, kEpilogueConvert = 1, kEpilogueCrt = 2 };
+
+struct Epilogue {
+    int mode;
+    // raw: D[m][col] int32, ld = columns
+    int32_t* raw;
+    uint32_t raw_ld;
+    // convert: residues[(op*r + k)*N + rem] = redc(S, p_k), for m = op*N + rem, g = k < r
+    uint32_t* residues;
+    const DevicePrime* primes;
+    uint32_t r, n;
+    // crt: dots[m * words + g] = S (u64), g < words
+    uint64_t* dots;
+    uint32_t words;
+};
+
+void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n,
+                         uint32_t limbs, uint32_t padded_limbs, cudaStream_t stream);
+void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv,
+                     uint2* zeta, cudaStream_t stream);
+void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,
+                            uint32_t k_bytes, uint8_t* out, cudaStream_t stream);
+void launch_crt_weights(const uint32_t* weights_words, uint32_t r, uint32_t padded_r, uint32_t words,
+                        uint32_t columns, uint8_t* out, cudaStream_t stream);
+void launch_gemm_simt(const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m, const uint8_t* b,
+                      uint32_t columns, uint32_t k_bytes, const Epilogue& epilogue, cudaStream_t stream);
+void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r,
+                        uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r,
+                      uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r,
+                        uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r,
+                      uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+
+struct ReduceParams {
+    const uint64_t* dots;     // [N][words]
+    uint32_t* out;            // [N][limbs]
+    const uint32_t* q;        // [limbs]
+    const uint32_t* minus_p;  // [limbs]  (-P) mod q
+    uint32_t n, limbs, words;
+    int32_t top_shift;
+    uint64_t mu_low;
+    uint32_t* error_flag;     // set nonzero if a coefficient needed more corrections than proven
+};
+void launch_reduce(const ReduceParams& params, cudaStream_t stream);
+
+}  // namespace negacyclic

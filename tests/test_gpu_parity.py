@@ -1,0 +1,200 @@
+"""Parity of the CUDA path (through the C ABI) with the reference checker and the oracle.
+
+Bit-exact everywhere: the product is integer arithmetic, the tolerance is 0.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import model
+from test_oracle import baseline_points, edge_pair, point_pairs, reference_points, as_array
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available(), "GPU tests need a CUDA device"
+    return t
+
+
+# ---------------------------------------------------------------- raw byte GEMM
+
+@pytest.mark.parametrize("m,n,k", [(128, 256, 128), (300, 520, 400), (1024, 768, 2048), (256, 512, 33024)])
+def test_tensor_gemm_matches_simt_and_numpy(m, n, k, fpc, torch):
+    gen = torch.Generator(device="cuda").manual_seed(m + n + k)
+    a = torch.randint(0, 256, (m, k), dtype=torch.uint8, device="cuda", generator=gen)
+    b = torch.randint(0, 256, (n, k), dtype=torch.uint8, device="cuda", generator=gen)
+    if k == 33024:  # the int32 accumulation bound: all-255 rows
+        a[0].fill_(255)
+        b[0].fill_(255)
+    outs = {}
+    lib = fpc.library()
+    for engine in (fpc.GEMM_SIMT, fpc.GEMM_TENSOR):
+        d = torch.full((m, n), -1, dtype=torch.int32, device="cuda")
+        status = lib.negacyclic_gemm_u8(a.data_ptr(), b.data_ptr(), d.data_ptr(), m, n, k, engine, None)
+        assert status == 0, fpc.last_error()
+        torch.cuda.synchronize()
+        outs[engine] = d.cpu().numpy()
+    want = a.cpu().numpy().astype(np.int64) @ b.cpu().numpy().astype(np.int64).T
+    assert np.array_equal(outs[fpc.GEMM_SIMT].astype(np.int64), want)
+    assert np.array_equal(outs[fpc.GEMM_TENSOR].astype(np.int64), want)
+
+
+# ---------------------------------------------------------------- reference checker points
+
+ENGINES = {"auto": 0, "simt": 1}
+
+
+@pytest.mark.parametrize("engine", sorted(ENGINES))
+@pytest.mark.parametrize("point", reference_points(), ids=lambda p: f"N{p['N']}_W{p['W']}_{p['kind']}")
+def test_reference_points_bit_exact(point, engine, fpc, inputs):
+    q, pairs = point_pairs(point)
+    limbs = point["L"]
+    q_arr = inputs.from_int(q, limbs)
+    with fpc.Plan(point["N"], point["W"], limbs, q_arr, gemm=ENGINES[engine]) as plan:
+        for (a, b), expect in zip(pairs, point["cases"]):
+            c = plan.run(as_array(a, limbs), as_array(b, limbs))
+            assert cases.sha256(c.tobytes()) == expect["c_sha256"]
+
+
+def test_plugin_interface_mirror(fpc, inputs):
+    """fherma_init / fherma_run / fherma_free as the reference's harness calls them."""
+    point = reference_points()[7]  # N=1024, W=512
+    q, pairs = point_pairs(point)
+    limbs = point["L"]
+    state = fpc.fherma_init(fpc.Point(point["N"], point["W"], limbs, inputs.from_int(q, limbs)))
+    try:
+        for (a, b), expect in zip(pairs, point["cases"]):
+            out = fpc.fherma_run(state, fpc.Inputs(as_array(a, limbs), as_array(b, limbs)))
+            assert out.c.shape == (point["N"], limbs)
+            assert cases.sha256(out.c.tobytes()) == expect["c_sha256"]
+        with pytest.raises(RuntimeError, match="wrong input size"):
+            fpc.fherma_run(state, fpc.Inputs(np.zeros((3, limbs), np.uint32), np.zeros((3, limbs), np.uint32)))
+    finally:
+        fpc.fherma_free(state)
+
+
+# ---------------------------------------------------------------- random odd q (the benchmark's kind of modulus)
+
+def baseline_cases(point, inputs):
+    n, limbs, seed = point["N"], point["L"], point["seed"]
+    q = inputs.random_modulus(limbs, seed)
+    edges = inputs.edge_operands(n, q) if any(not e["label"].startswith("seed") for e in point["cases"]) else {}
+    for entry in point["cases"]:
+        label = entry["label"]
+        if label.startswith("seed"):
+            _, a, b = inputs.instance(n, limbs, seed, int(label.split("index")[1]))
+        else:
+            x, y = edge_pair(inputs, label)
+            a, b = edges[x], edges[y]
+        yield label, q, a, b, entry
+
+
+@pytest.mark.parametrize("point", [p for p in baseline_points() if p["N"] * p["L"] <= 4096 * 64],
+                         ids=lambda p: f"N{p['N']}_L{p['L']}")
+@pytest.mark.parametrize("engine", sorted(ENGINES))
+def test_random_modulus_config_bit_exact(point, engine, fpc, inputs):
+    plan = None
+    for label, q, a, b, entry in baseline_cases(point, inputs):
+        if plan is None:
+            plan = fpc.Plan(point["N"], 32 * point["L"], point["L"], q, gemm=ENGINES[engine])
+        c = plan.run(a, b)
+        assert cases.sha256(c.tobytes()) == entry["c_sha256"], label
+    plan.close()
+
+
+@pytest.mark.parametrize("n,limbs,split", [(1, 1, 0), (2, 3, 0), (8, 2, 2), (64, 1, 0), (128, 29, 0),
+                                           (256, 40, 2), (512, 33, 4), (2048, 17, 0), (4096, 70, 0),
+                                           (8192, 32, 0), (16384, 9, 0)])
+def test_random_points_against_oracle(n, limbs, split, fpc, inputs, oracle):
+    for index in range(2):
+        q, a, b = inputs.instance(n, limbs, 1000 + n + limbs, index)
+        want = oracle.kronecker(q, a, b)
+        for engine in (0, 1):
+            with fpc.Plan(n, 32 * limbs, limbs, q, split=split, gemm=engine) as plan:
+                got = plan.run(a, b)
+            assert np.array_equal(got, want), (n, limbs, split, engine, index)
+
+
+def test_small_moduli(fpc, inputs, oracle):
+    """q of one or two limbs, including q below a prime and q = 2, 3."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    for qv in (2, 3, 5, 65537, 0xFFFFFFFF, (1 << 31) - 1, (1 << 61) - 1, (1 << 64) - 59):
+        limbs = 1 if qv < (1 << 32) else 2
+        q = inputs.from_int(qv, limbs)
+        a = inputs.random_operand(rng, 512, q)
+        b = inputs.random_operand(rng, 512, q)
+        with fpc.Plan(512, 32 * limbs, limbs, q) as plan:
+            assert np.array_equal(plan.run(a, b), oracle.kronecker(q, a, b)), qv
+
+
+# ---------------------------------------------------------------- stage-by-stage against the model
+
+@pytest.mark.parametrize("n,limbs,split", [(256, 4, 2), (512, 33, 1), (1024, 2, 4)])
+def test_stages_match_model(n, limbs, split, fpc, inputs):
+    q, a, b = inputs.instance(n, limbs, 77, 0)
+    qi = inputs.to_int(q)
+    ref = model.stages(model.make_plan(n, limbs, qi, split), inputs.poly_to_ints(a), inputs.poly_to_ints(b))
+    with fpc.Plan(n, 32 * limbs, limbs, q, split=split) as plan:
+        info = plan.info()
+        c = plan.run(a, b)
+        crt_in = np.frombuffer(plan.debug_read(1), np.uint32).reshape(n, info["padded_primes"])
+        dots = np.frombuffer(plan.debug_read(2), np.uint64).reshape(n, info["words"])
+    r = info["primes"]
+    v = np.array(ref["v"], dtype=np.uint32).T  # [n][r]
+    assert np.array_equal(crt_in[:, :r], v)
+    assert not crt_in[:, r:].any()
+    assert np.array_equal(dots, np.array(ref["dots"], dtype=np.uint64))
+    assert inputs.poly_to_ints(c) == ref["c"]
+
+
+# ---------------------------------------------------------------- device-resident entry point
+
+def test_run_device_matches_run(fpc, inputs, torch):
+    n, limbs = 4096, 64
+    q, a, b = inputs.instance(n, limbs, 0, 0)
+    with fpc.Plan(n, 32 * limbs, limbs, q) as plan:
+        host = plan.run(a, b)
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(b.view(np.int32)).cuda()
+        dc = torch.empty_like(da)
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(2):  # twice: internal buffers are reused
+            plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), stream)
+            torch.cuda.synchronize()
+            assert np.array_equal(dc.cpu().numpy().view(np.uint32), host)
+
+
+# ---------------------------------------------------------------- full-size configurations
+
+def big_points():
+    return [p for p in baseline_points() if p["N"] * p["L"] > 4096 * 64]
+
+
+@pytest.mark.parametrize("point", big_points(), ids=lambda p: f"N{p['N']}_L{p['L']}")
+def test_full_size_against_reference_hash_and_properties(point, fpc, inputs, oracle):
+    """Bit-exact at N=32768/L=868 and N=65536/L=1747 against the reference checker's hash,
+    plus size-independent checks: direct coefficient sums, and a*(X b) = X (a b)."""
+    n, limbs = point["N"], point["L"]
+    ((label, q, a, b, entry),) = list(baseline_cases(point, inputs))
+    with fpc.Plan(n, 32 * limbs, limbs, q) as plan:
+        info = plan.info()
+        assert info["gemm"] == 3, info  # both byte GEMMs on tensor cores
+        c = plan.run(a, b)
+        assert cases.sha256(c.tobytes()) == entry["c_sha256"], label
+        for i in (0, n - 1):
+            assert np.array_equal(oracle.schoolbook_at(q, a, b, i)[0], c[i]), i
+        # negacyclic shift: X*b has b_{N-1} negated at index 0
+        qi = inputs.to_int(q)
+        xb = np.roll(b, 1, axis=0)
+        xb[0] = inputs.from_int((qi - inputs.to_int(b[-1])) % qi, limbs)
+        shifted = plan.run(a, xb)
+    assert np.array_equal(shifted[1:], c[:-1])
+    assert inputs.to_int(shifted[0]) == (qi - inputs.to_int(c[-1])) % qi
