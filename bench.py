@@ -68,7 +68,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms while running."""
 
     FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
               "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
@@ -81,10 +81,13 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={','.join(self.FIELDS)}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            deadline = time.time() + 3.0  # start timing only once samples are flowing
+            while not self.rows and time.time() < deadline:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
@@ -176,14 +179,15 @@ def run_b200(args):
     import torch.distributed as dist
 
     world, rank, local = distributed()
+    n_coeff, limbs = args.n, args.limbs
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=600))
     fpc = _load("fpc_b200", os.path.join(PACKAGE_DIR, "__init__.py"), PACKAGE_DIR)
     inputs = load_inputs()
-    q, a, b = inputs.instance(N, LIMBS, SEED, rank)
-    plan = fpc.Plan(N, 32 * LIMBS, LIMBS, q, device=local)
+    q, a, b = inputs.instance(n_coeff, limbs, SEED, rank)
+    plan = fpc.Plan(n_coeff, 32 * limbs, limbs, q, device=local)
     info = plan.info()
     stream = torch.cuda.Stream()
     da = torch.from_numpy(a.view(np.int32)).cuda()
@@ -203,12 +207,12 @@ def run_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # --- device-resident products
-    for _ in range(args.warmup):
-        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
-    barrier()
+    # --- device-resident products (clocks sampled from the warm-up through the timed region)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        for _ in range(args.warmup):
+            plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
+        barrier()
         start.record(stream)
         for _ in range(args.steps):
             plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
@@ -225,6 +229,15 @@ def run_b200(args):
             stage_ms[name] += ms / args.steps
 
     # --- end to end through the host-facing C ABI, pinned host buffers
+    if args.device_only:
+        plan.close()
+        if rank == 0:
+            print(json.dumps({"workload": f"N={n_coeff} L={limbs}", "value": value, "unit": "products/s",
+                              "ms_per_step": device_ms / args.steps,
+                              "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()}}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     pa = torch.from_numpy(a.view(np.int32)).pin_memory()
     pb = torch.from_numpy(b.view(np.int32)).pin_memory()
     pc = torch.empty_like(pa).pin_memory()
@@ -245,8 +258,8 @@ def run_b200(args):
     # --- roofline of the conversion GEMM: 2 ops per byte MAC, M=2N rows, K=4L bytes, 4r weight columns
     hbm_gbs, bf16_tflops, source = peaks()
     int8_peak = 2 * bf16_tflops  # dense int8 = 2x dense bf16 on B200
-    conv_ops = 2.0 * (2 * N) * (4 * LIMBS) * (4 * info["primes"])
-    crt_ops = 2.0 * N * (4 * info["primes"]) * (4 * info["words"])
+    conv_ops = 2.0 * (2 * n_coeff) * (4 * limbs) * (4 * info["primes"])
+    crt_ops = 2.0 * n_coeff * (4 * info["primes"]) * (4 * info["words"])
     conv_tops = conv_ops / (stage_ms["convert"] / 1000) / 1e12
     roofline = {
         "bound": "tensor", "kernel": "gemm_tc_kernel (conversion, tcgen05 kind::i8)",
@@ -291,11 +304,16 @@ def run_b200(args):
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    parser.add_argument("--workload", default=f"{N},{LIMBS}",
+                        help="N,L of a smaller case for profiling (the benchmark line is N=65536,L=1747)")
+    parser.add_argument("--device-only", action="store_true",
+                        help="device-resident products and stage times only (profiling runs)")
     args = parser.parse_args()
+    args.n, args.limbs = (int(x) for x in args.workload.split(","))
     if args.impl == "reference":
         run_reference(args)
     else:

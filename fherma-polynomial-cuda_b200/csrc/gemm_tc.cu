@@ -12,11 +12,12 @@
 // Exactness: each accumulator is a sum of K products of bytes, K * 255^2 < 2^31
 // for K <= 33024 (checked by the plan), so s32 accumulation is exact.
 //
-// Warp roles (128 threads, one warpgroup): warp 0 lane 0 = TMA producer,
-// warp 1 lane 0 = MMA issuer, warp 2 = TMEM allocator; all four warps run the
-// epilogue (warp w owns TMEM lanes / tile rows 32w..32w+31). Every mbarrier
-// wait is bounded (~2 s of SM clock); on timeout the kernel records an error
-// bit, still commits/waits what it issued, frees TMEM and returns.
+// Persistent (one CTA per SM) and warp-specialised: warp 0 = TMA producer,
+// warp 1 = MMA issuer and TMEM owner (two 256-column accumulators), warps 2-5 =
+// epilogue, so the epilogue of one tile overlaps the MMAs of the next. Every
+// mbarrier wait is bounded (~2 s of SM clock); on timeout the kernel records an
+// error bit, tells the other roles to stop, waits for what it issued, frees
+// TMEM and returns.
 #include <cuda.h>
 
 #include <cstdio>
@@ -32,10 +33,12 @@ constexpr uint32_t kStages = 4;
 constexpr uint32_t kATileBytes = kBlockM * kBlockK;                // 16 KB
 constexpr uint32_t kBTileBytes = kBlockN * kBlockK;                // 32 KB
 constexpr uint32_t kStageBytes = kATileBytes + kBTileBytes;
-constexpr uint32_t kTmemColumns = 256;
+constexpr uint32_t kAccColumns = 256;                            // one 128 x 256 s32 accumulator
+constexpr uint32_t kEpilogueWarps = 4;
+constexpr uint32_t kThreads = 64 + 32 * kEpilogueWarps;
 constexpr uint32_t kGroupM = 16;                                   // m-tiles per raster group (L2 reuse of B)
 constexpr long long kTimeoutCycles = 4000000000ll;
-constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers, TMEM slot*/;
 
 __device__ uint32_t g_tc_error;
 
@@ -144,46 +147,57 @@ struct TileShape {
     RowMap rows;
 };
 
-__global__ void __launch_bounds__(128, 1) gemm_tc_kernel(const __grid_constant__ CUtensorMap a_map,
-                                                         const __grid_constant__ CUtensorMap b_map, TileShape shape,
-                                                         Epilogue epi) {
+// Tile index -> (m tile, n tile) in groups of kGroupM m-tiles, m fastest, so the
+// CTAs running at the same time share B tiles (and their A tiles stay in L2).
+__device__ __forceinline__ void tile_coords(uint32_t tile, const TileShape& shape, uint32_t& m_tile,
+                                            uint32_t& n_tile) {
+    const uint32_t span = kGroupM * shape.n_tiles;
+    const uint32_t group = tile / span, within = tile - group * span;
+    const uint32_t first_m = group * kGroupM;
+    const uint32_t rows_in_group = min(kGroupM, shape.m_tiles - first_m);
+    m_tile = first_m + within % rows_in_group;
+    n_tile = within / rows_in_group;
+}
+
+// Persistent, warp-specialised GEMM: each CTA walks tiles blockIdx.x, +gridDim.x, ...
+//   warp 0 (one thread)  TMA producer over a kStages-deep shared-memory ring
+//   warp 1 (one thread)  MMA issuer; the whole warp allocates / frees 512 TMEM columns
+//   warps 2-5            epilogue; two 256-column accumulators alternate between tiles,
+//                        so tile i's epilogue overlaps tile i+1's MMAs
+__global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_constant__ CUtensorMap a_map,
+                                                              const __grid_constant__ CUtensorMap b_map,
+                                                              TileShape shape, Epilogue epi) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* a_smem = smem;
     uint8_t* b_smem = smem + kStages * kATileBytes;
     uint64_t* full = reinterpret_cast<uint64_t*>(b_smem + kStages * kBTileBytes);
     uint64_t* empty = full + kStages;
-    uint64_t* done = empty + kStages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* acc_full = empty + kStages;  // [2] MMA -> epilogue
+    uint64_t* acc_empty = acc_full + 2;    // [2] epilogue -> MMA
+    uint64_t* drain = acc_empty + 2;       // MMA warp's final completion
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile uint32_t* abort_flag = tmem_slot + 1;
 
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-
-    // grouped raster: kGroupM m-tiles share each B tile while it is hot in L2
-    const uint32_t span = kGroupM * shape.n_tiles;
-    const uint32_t group = blockIdx.x / span, within = blockIdx.x - group * span;
-    const uint32_t first_m = group * kGroupM;
-    const uint32_t rows_in_group = min(kGroupM, shape.m_tiles - first_m);
-    const uint32_t m_tile = first_m + within % rows_in_group, n_tile = within / rows_in_group;
-    const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
-    // A-map coordinates of the tile's first row
-    uint32_t a_t = 0, a_row = row0;
-    if (shape.rows.mode == kRowsSplit) {
-        uint32_t op = row0 / shape.rows.n, rem = row0 - op * shape.rows.n;
-        a_t = rem / shape.rows.n_sub;
-        a_row = op * shape.rows.n_sub + (rem - a_t * shape.rows.n_sub);
-    }
+    const uint32_t tiles = shape.m_tiles * shape.n_tiles;
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < kStages; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (uint32_t a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], kEpilogueWarps);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 2) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemColumns)
+                     "r"(2 * kAccColumns)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -191,91 +205,146 @@ __global__ void __launch_bounds__(128, 1) gemm_tc_kernel(const __grid_constant__
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    bool ok = true;
 
-    if (warp == 0 && lane == 0) {
-        // producer
-        uint32_t issued = 0;
-        for (uint32_t ks = 0; ks < shape.k_tiles; ++ks) {
-            const uint32_t s = ks % kStages, round = ks / kStages;
-            if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
-                ok = false;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            uint32_t step = 0, issued = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+                uint32_t m_tile, n_tile;
+                tile_coords(tile, shape, m_tile, n_tile);
+                const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
+                uint32_t a_t = 0, a_row = row0;
+                if (shape.rows.mode == kRowsSplit) {
+                    uint32_t op = row0 / shape.rows.n, rem = row0 - op * shape.rows.n;
+                    a_t = rem / shape.rows.n_sub;
+                    a_row = op * shape.rows.n_sub + (rem - a_t * shape.rows.n_sub);
+                }
+                for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
+                    const uint32_t s = step % kStages, round = step / kStages;
+                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], kStageBytes);
+                    tma_load_3d(a_smem + s * kATileBytes, &a_map, &full[s], int(ks * kBlockK), int(a_t), int(a_row));
+                    tma_load_2d(b_smem + s * kBTileBytes, &b_map, &full[s], int(ks * kBlockK), int(col0));
+                    issued = step + 1;
+                }
             }
-            mbar_expect_tx(&full[s], kStageBytes);
-            tma_load_3d(a_smem + s * kATileBytes, &a_map, &full[s], int(ks * kBlockK), int(a_t), int(a_row));
-            tma_load_2d(b_smem + s * kBTileBytes, &b_map, &full[s], int(ks * kBlockK), int(col0));
-            issued = ks + 1;
+            if (!ok) {
+                *abort_flag = 1;
+                atomicOr(&g_tc_error, 1u);
+                // let the loads already issued land before the CTA can exit
+                for (uint32_t st = (issued > kStages ? issued - kStages : 0); st < issued; ++st)
+                    mbar_wait(&full[st % kStages], (st / kStages) & 1);
+            }
         }
-        if (!ok) {
-            // let the loads already issued land before the CTA can exit
-            for (uint32_t ks = (issued > kStages ? issued - kStages : 0); ks < issued; ++ks)
-                mbar_wait(&full[ks % kStages], (ks / kStages) & 1);
-            atomicOr(&g_tc_error, 1u);
-        }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        for (uint32_t ks = 0; ks < shape.k_tiles; ++ks) {
-            const uint32_t s = ks % kStages, round = ks / kStages;
-            if (!mbar_wait(&full[s], round & 1)) {
-                ok = false;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            uint32_t step = 0, local = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++local) {
+                const uint32_t acc = local & 1, use = local >> 1;
+                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t d_tmem = tmem + acc * kAccColumns;
+                for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
+                    const uint32_t s = step % kStages, round = step / kStages;
+                    if (*abort_flag || !mbar_wait(&full[s], round & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t a_addr = smem_u32(a_smem + s * kATileBytes);
+                    const uint32_t b_addr = smem_u32(b_smem + s * kBTileBytes);
+#pragma unroll
+                    for (uint32_t kk = 0; kk < kBlockK / 32; ++kk)
+                        mma_i8(d_tmem, smem_descriptor(a_addr + kk * 32), smem_descriptor(b_addr + kk * 32),
+                               (ks | kk) != 0 ? 1u : 0u);
+                    mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+                }
+                if (ok) mma_commit(&acc_full[acc]);  // accumulator complete
+            }
+            if (!ok) {
+                *abort_flag = 1;
                 atomicOr(&g_tc_error, 2u);
+            }
+            mma_commit(drain);  // arrives once every MMA issued above has completed
+            if (!mbar_wait(drain, 0)) atomicOr(&g_tc_error, 8u);
+        }
+    } else {
+        // ---------------- epilogue: warp w reads TMEM lanes 32*(w%4).. (rows of the tile)
+        const uint32_t quarter = warp & 3;
+        uint32_t local = 0;
+        for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++local) {
+            const uint32_t acc = local & 1, use = local >> 1;
+            uint32_t m_tile, n_tile;
+            tile_coords(tile, shape, m_tile, n_tile);
+            const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
+            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1);
+            have = __all_sync(0xffffffffu, have);
+            if (!have) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicOr(&g_tc_error, 4u);
+                }
                 break;
             }
             fence_after();
-            const uint32_t a_addr = smem_u32(a_smem + s * kATileBytes), b_addr = smem_u32(b_smem + s * kBTileBytes);
-#pragma unroll
-            for (uint32_t kk = 0; kk < kBlockK / 32; ++kk)
-                mma_i8(tmem, smem_descriptor(a_addr + kk * 32), smem_descriptor(b_addr + kk * 32),
-                       (ks | kk) != 0 ? 1u : 0u);
-            mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
-        }
-        mma_commit(done);  // arrives when every MMA issued above has completed
-    }
-    __syncwarp();
-
-    // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes)
-    const bool have = mbar_wait(done, 0);
-    if (!have && lane == 0) atomicOr(&g_tc_error, 4u);
-    fence_after();
-    const uint32_t row = row0 + warp * 32 + lane;
-    const bool row_ok = row < shape.m;
-    if (have) {
-        for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
-            const uint32_t c_base = col0 + chunk * 32;
-            if (c_base >= shape.columns) break;  // warp-uniform
-            uint32_t v[32];
-            tmem_load32(tmem + ((warp * 32) << 16) + chunk * 32, v);
-            if (!row_ok) continue;
-            if (epi.mode == kEpilogueRaw) {
-                int32_t* out = epi.raw + size_t(row) * epi.raw_ld;
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (c_base + j < shape.columns) out[c_base + j] = int32_t(v[j]);
-                continue;
+            const uint32_t row = row0 + quarter * 32 + lane;
+            const bool row_ok = row < shape.m;
+            uint32_t op = 0, rem = row;
+            if (epi.mode == kEpilogueConvert) {
+                op = row / epi.n;
+                rem = row - op * epi.n;
             }
+            const uint32_t t_base = tmem + acc * kAccColumns + ((quarter * 32) << 16);
+            for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
+                const uint32_t c_base = col0 + chunk * 32;
+                if (c_base >= shape.columns) break;  // warp-uniform
+                uint32_t v[32];
+                tmem_load32(t_base + chunk * 32, v);
+                if (!row_ok) continue;
+                if (epi.mode == kEpilogueRaw) {
+                    int32_t* out = epi.raw + size_t(row) * epi.raw_ld;
 #pragma unroll
-            for (int g = 0; g < 8; ++g) {
-                const uint32_t group_index = c_base / 4 + g;
-                uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
-                             (uint64_t(v[4 * g + 3]) << 24);
-                if (epi.mode == kEpilogueConvert) {
-                    if (group_index < epi.r) {
-                        const DevicePrime f = epi.primes[group_index];
-                        uint32_t op = row / epi.n, rem = row - op * epi.n;
-                        epi.residues[(size_t(op) * epi.r + group_index) * epi.n + rem] = redc(s, f.p, f.pinv);
+                    for (int j = 0; j < 32; ++j)
+                        if (c_base + j < shape.columns) out[c_base + j] = int32_t(v[j]);
+                    continue;
+                }
+#pragma unroll
+                for (int g = 0; g < 8; ++g) {
+                    const uint32_t group_index = c_base / 4 + g;
+                    uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) +
+                                 (uint64_t(v[4 * g + 2]) << 16) + (uint64_t(v[4 * g + 3]) << 24);
+                    if (epi.mode == kEpilogueConvert) {
+                        if (group_index < epi.r) {
+                            const DevicePrime f = epi.primes[group_index];
+                            epi.residues[(size_t(op) * epi.r + group_index) * epi.n + rem] = redc(s, f.p, f.pinv);
+                        }
+                    } else if (group_index < epi.words) {
+                        epi.dots[size_t(row) * epi.words + group_index] = s;
                     }
-                } else if (group_index < epi.words) {
-                    epi.dots[size_t(row) * epi.words + group_index] = s;
                 }
             }
+            // every tcgen05.ld of this warp has completed (tmem_load32 waits): release the accumulator
+            fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[acc])) : "memory");
         }
     }
+    __syncwarp();
     fence_before();
     __syncthreads();
-    if (warp == 2) {
+    if (warp == 1) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kAccColumns)
                      : "memory");
     }
 }
@@ -373,14 +442,19 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     plan.k_tiles = (k_bytes + kBlockK - 1) / kBlockK;
     plan.rows = rows;
     plan.error_flag = tensor_gemm_error_flag();
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    plan.sm_count = sms > 0 ? uint32_t(sms) : 148;
     plan.ready = true;
     return true;
 }
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {
     TileShape shape{plan.m, plan.columns, plan.k_tiles, plan.m_tiles, plan.n_tiles, plan.rows};
-    gemm_tc_kernel<<<plan.m_tiles * plan.n_tiles, 128, kSmemBytes, stream>>>(plan.a_map, plan.b_map, shape,
-                                                                               epilogue);
+    const uint32_t tiles = plan.m_tiles * plan.n_tiles;
+    const uint32_t grid = tiles < plan.sm_count ? tiles : plan.sm_count;
+    gemm_tc_kernel<<<grid, kThreads, kSmemBytes, stream>>>(plan.a_map, plan.b_map, shape, epilogue);
 }
 
 }  // namespace negacyclic

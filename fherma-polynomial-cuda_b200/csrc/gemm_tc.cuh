@@ -16,6 +16,7 @@ struct TensorGemmPlan {
     uint32_t m_tiles = 0, n_tiles = 0, k_tiles = 0;
     RowMap rows{};
     uint32_t* error_flag = nullptr;  // device word set when a pipeline wait times out
+    uint32_t sm_count = 148;          // persistent grid size
     bool ready = false;
 };
 

@@ -10,6 +10,8 @@
 //                                  zeta psi^(2 brv(m)+1) (evaluation point at output m)
 #include "kernels.cuh"
 
+#include <algorithm>
+
 namespace negacyclic {
 
 namespace {
@@ -200,6 +202,152 @@ __global__ void __launch_bounds__(512) ntt_inverse_kernel(uint32_t* residues, co
         __syncthreads();
     }
     for (uint32_t j = threadIdx.x; j < n_sub; j += blockDim.x) data[j] = shoup(x[j], f.finish, f.finish_q, f.p);
+}
+
+// ---------------------------------------------------------------------------
+// Register-blocked NTT for N' >= 256: 16 values per thread (N'/16 threads),
+// up to four butterfly stages per pass between shared-memory exchanges.
+// A pass of R stages on group g (2^R values spaced t_min apart, t_min = the
+// smallest half-size in the pass) covers indices base + k*t_min, k < 2^R, with
+// base = (g / t_min) * 2^R * t_min + g % t_min.
+
+constexpr uint32_t kPerThread = 16;
+
+__device__ __forceinline__ uint32_t padded(uint32_t i) { return i + (i >> 5); }  // bank-conflict padding
+
+// Cooley-Tukey stages with half-sizes t_min*2^(R-1) .. t_min (forward, merged psi twiddles).
+template <int R>
+__device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t base, uint32_t log_t_min, uint32_t log_n,
+                                          const uint2* __restrict__ table, uint32_t p) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int half = 1 << (R - 1 - r);
+        const uint32_t log_t = log_t_min + (R - 1 - r);  // this stage's half-size t = 2^log_t
+        const uint32_t m = 1u << (log_n - 1 - log_t);     // number of groups: n / (2t)
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+            if (k & half) continue;
+            const uint32_t j = base + (uint32_t(k) << log_t_min);
+            const uint2 w = __ldg(&table[m + (j >> (log_t + 1))]);
+            const uint32_t u = x[k], v = shoup(x[k + half], w.x, w.y, p);
+            x[k] = add_mod(u, v, p);
+            x[k + half] = sub_mod(u, v, p);
+        }
+    }
+}
+
+// Gentleman-Sande stages with half-sizes t_min .. t_min*2^(R-1) (inverse).
+template <int R>
+__device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t base, uint32_t log_t_min, uint32_t log_n,
+                                          const uint2* __restrict__ table, uint32_t p) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int half = 1 << r;
+        const uint32_t log_t = log_t_min + r;
+        const uint32_t h = 1u << (log_n - 1 - log_t);
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+            if (k & half) continue;
+            const uint32_t j = base + (uint32_t(k) << log_t_min);
+            const uint2 w = __ldg(&table[h + (j >> (log_t + 1))]);
+            const uint32_t u = x[k], v = x[k + half];
+            x[k] = add_mod(u, v, p);
+            x[k + half] = shoup(sub_mod(u, v, p), w.x, w.y, p);
+        }
+    }
+}
+
+// One pass of R stages over all of this thread's groups. src/dst are shared
+// (padded index) or global (plain index); `scale` multiplies values stored to global.
+template <int R, bool kForward, bool kFromGlobal, bool kToGlobal>
+__device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, uint32_t log_t_min, uint32_t log_n,
+                                         const uint2* __restrict__ table, uint32_t p, bool scale, uint32_t f,
+                                         uint32_t f_q) {
+    constexpr int G = kPerThread >> R;  // groups per thread
+    const uint32_t threads = blockDim.x;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const uint32_t group = threadIdx.x + g * threads;
+        const uint32_t off = group & ((1u << log_t_min) - 1);
+        const uint32_t base = ((group >> log_t_min) << (log_t_min + R)) + off;
+        uint32_t x[1 << R];
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+            const uint32_t i = base + (uint32_t(k) << log_t_min);
+            x[k] = kFromGlobal ? src[i] : src[padded(i)];
+        }
+        if (kForward)
+            ct_stages<R>(x, base, log_t_min, log_n, table, p);
+        else
+            gs_stages<R>(x, base, log_t_min, log_n, table, p);
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+            const uint32_t i = base + (uint32_t(k) << log_t_min);
+            uint32_t value = x[k];
+            if (kToGlobal && scale) value = shoup(value, f, f_q, p);
+            if (kToGlobal)
+                dst[i] = value;
+            else
+                dst[padded(i)] = value;
+        }
+    }
+}
+
+template <bool kForward, bool kFromGlobal, bool kToGlobal>
+__device__ __forceinline__ void ntt_pass_r(int R, const uint32_t* src, uint32_t* dst, uint32_t log_t_min,
+                                           uint32_t log_n, const uint2* __restrict__ table, uint32_t p, bool scale,
+                                           uint32_t f, uint32_t f_q) {
+    switch (R) {
+        case 4: ntt_pass<4, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
+        case 3: ntt_pass<3, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
+        case 2: ntt_pass<2, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
+        default: ntt_pass<1, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
+    }
+}
+
+// Whole transform of `data` (length 2^log_n, log_n >= 8) in place: passes of four
+// stages, then the remainder; forward runs half-sizes large -> small, inverse
+// small -> large and multiplies its output by (f, f_q).
+template <bool kForward>
+__device__ __forceinline__ void ntt_blocked(uint32_t* data, uint32_t* xs, uint32_t log_n, const uint2* table,
+                                            uint32_t p, uint32_t f, uint32_t f_q) {
+    const uint32_t passes = (log_n + 3) / 4;
+    uint32_t done = 0;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const int R = int(min(4u, log_n - done));
+        // forward: the pass's smallest half-size is n / 2^(done + R); inverse: 2^done
+        const uint32_t log_t_min = kForward ? log_n - done - R : done;
+        const bool first = pass == 0, last = pass + 1 == passes;
+        if (first)
+            ntt_pass_r<kForward, true, false>(R, data, xs, log_t_min, log_n, table, p, false, f, f_q);
+        else if (last)
+            ntt_pass_r<kForward, false, true>(R, xs, data, log_t_min, log_n, table, p, !kForward, f, f_q);
+        else
+            ntt_pass_r<kForward, false, false>(R, xs, xs, log_t_min, log_n, table, p, false, f, f_q);
+        done += R;
+        if (!last) __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(512) ntt_forward_blocked_kernel(uint32_t* residues,
+                                                                  const DevicePrime* __restrict__ primes,
+                                                                  const uint2* __restrict__ fwd, uint32_t r,
+                                                                  uint32_t n, uint32_t n_sub, uint32_t log_n) {
+    extern __shared__ uint32_t xs[];
+    const uint32_t t_index = blockIdx.x, k = blockIdx.y, op = blockIdx.z;
+    uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * n_sub;
+    ntt_blocked<true>(data, xs, log_n, fwd + size_t(k) * n_sub, primes[k].p, 0, 0);
+}
+
+__global__ void __launch_bounds__(512) ntt_inverse_blocked_kernel(uint32_t* residues,
+                                                                  const DevicePrime* __restrict__ primes,
+                                                                  const uint2* __restrict__ inv, uint32_t r,
+                                                                  uint32_t n, uint32_t n_sub, uint32_t log_n) {
+    extern __shared__ uint32_t xs[];
+    const uint32_t v_index = blockIdx.x, k = blockIdx.y;
+    const DevicePrime f = primes[k];
+    uint32_t* data = residues + size_t(k) * n + size_t(v_index) * n_sub;
+    ntt_blocked<false>(data, xs, log_n, inv + size_t(k) * n_sub, f.p, f.finish, f.finish_q);
 }
 
 // C_v = sum_{t+u=v} A_t B_u + zeta * sum_{t+u=v+s} A_t B_u at every evaluation point,
@@ -439,6 +587,12 @@ static uint32_t ntt_threads(uint32_t n_sub) {
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r, uint32_t n,
                         uint32_t n_sub, uint32_t split, cudaStream_t stream) {
     dim3 grid(split, r, 2);
+    if (n_sub >= 256) {
+        const size_t smem = (n_sub + n_sub / 32) * sizeof(uint32_t);
+        ntt_forward_blocked_kernel<<<grid, n_sub / kPerThread, smem, stream>>>(residues, primes, fwd, r, n, n_sub,
+                                                                                log2_u32(n_sub));
+        return;
+    }
     ntt_forward_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, fwd, r, n,
                                                                                           n_sub);
 }
@@ -446,6 +600,12 @@ void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uin
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r, uint32_t n,
                         uint32_t n_sub, uint32_t split, cudaStream_t stream) {
     dim3 grid(split, r);
+    if (n_sub >= 256) {
+        const size_t smem = (n_sub + n_sub / 32) * sizeof(uint32_t);
+        ntt_inverse_blocked_kernel<<<grid, n_sub / kPerThread, smem, stream>>>(residues, primes, inv, r, n, n_sub,
+                                                                                log2_u32(n_sub));
+        return;
+    }
     ntt_inverse_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, inv, r, n,
                                                                                           n_sub);
 }
@@ -469,9 +629,13 @@ void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, ui
 }
 
 void launch_reduce(const ReduceParams& params, cudaStream_t stream) {
-    const uint32_t warps = 8;
     const uint32_t stride = (params.words + 1 + 31) / 32 * 32;
+    // up to 8 warps (coefficients) per block, each with `stride` words of shared memory
+    constexpr size_t kSmemBudget = 200 * 1024;
+    uint32_t warps = uint32_t(std::min<size_t>(8, std::max<size_t>(1, kSmemBudget / (stride * sizeof(uint32_t)))));
     const size_t smem = size_t(warps) * stride * sizeof(uint32_t);
+    if (smem > 48 * 1024)  // per device; cheap enough to repeat
+        cudaFuncSetAttribute(reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBudget));
     uint32_t blocks = (params.n + warps - 1) / warps;
     if (blocks > 148u * 8) blocks = 148u * 8;
     reduce_kernel<<<blocks, warps * 32, smem, stream>>>(params, stride);

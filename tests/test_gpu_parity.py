@@ -112,7 +112,7 @@ def test_random_modulus_config_bit_exact(point, engine, fpc, inputs):
 
 @pytest.mark.parametrize("n,limbs,split", [(1, 1, 0), (2, 3, 0), (8, 2, 2), (64, 1, 0), (128, 29, 0),
                                            (256, 40, 2), (512, 33, 4), (2048, 17, 0), (4096, 70, 0),
-                                           (8192, 32, 0), (16384, 9, 0)])
+                                           (8192, 32, 0), (16384, 9, 0), (1024, 1747, 0), (256, 3000, 0)])
 def test_random_points_against_oracle(n, limbs, split, fpc, inputs, oracle):
     for index in range(2):
         q, a, b = inputs.instance(n, limbs, 1000 + n + limbs, index)
