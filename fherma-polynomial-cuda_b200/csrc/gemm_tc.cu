@@ -36,7 +36,6 @@ constexpr uint32_t kStageBytes = kATileBytes + kBTileBytes;
 constexpr uint32_t kAccColumns = 256;                            // one 128 x 256 s32 accumulator
 constexpr uint32_t kEpilogueWarps = 4;
 constexpr uint32_t kThreads = 64 + 32 * kEpilogueWarps;
-constexpr uint32_t kGroupM = 16;                                   // m-tiles per raster group (L2 reuse of B)
 constexpr long long kTimeoutCycles = 4000000000ll;
 constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers, TMEM slot*/;
 
@@ -143,18 +142,18 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&v)[32]) {
 }
 
 struct TileShape {
-    uint32_t m, columns, k_tiles, m_tiles, n_tiles;
+    uint32_t m, columns, k_tiles, m_tiles, n_tiles, group_m;
     RowMap rows;
 };
 
-// Tile index -> (m tile, n tile) in groups of kGroupM m-tiles, m fastest, so the
+// Tile index -> (m tile, n tile) in groups of group_m m-tiles, m fastest, so the
 // CTAs running at the same time share B tiles (and their A tiles stay in L2).
 __device__ __forceinline__ void tile_coords(uint32_t tile, const TileShape& shape, uint32_t& m_tile,
                                             uint32_t& n_tile) {
-    const uint32_t span = kGroupM * shape.n_tiles;
+    const uint32_t span = shape.group_m * shape.n_tiles;
     const uint32_t group = tile / span, within = tile - group * span;
-    const uint32_t first_m = group * kGroupM;
-    const uint32_t rows_in_group = min(kGroupM, shape.m_tiles - first_m);
+    const uint32_t first_m = group * shape.group_m;
+    const uint32_t rows_in_group = min(shape.group_m, shape.m_tiles - first_m);
     m_tile = first_m + within % rows_in_group;
     n_tile = within / rows_in_group;
 }
@@ -215,11 +214,12 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 uint32_t m_tile, n_tile;
                 tile_coords(tile, shape, m_tile, n_tile);
                 const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
-                uint32_t a_t = 0, a_row = row0;
+                // A-map coordinates of the tile's first row: (t, op*N' + j) or (0, first + row0)
+                uint32_t a_t = 0, a_row = shape.rows.first + row0;
                 if (shape.rows.mode == kRowsSplit) {
-                    uint32_t op = row0 / shape.rows.n, rem = row0 - op * shape.rows.n;
-                    a_t = rem / shape.rows.n_sub;
-                    a_row = op * shape.rows.n_sub + (rem - a_t * shape.rows.n_sub);
+                    uint32_t op, j;
+                    shape.rows.decompose(row0, op, a_t, j);
+                    a_row = op * shape.rows.n_sub + j;
                 }
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kStages, round = step / kStages;
@@ -297,12 +297,15 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 break;
             }
             fence_after();
-            const uint32_t row = row0 + quarter * 32 + lane;
+            const uint32_t row = row0 + quarter * 32 + lane;  // GEMM row of this lane
             const bool row_ok = row < shape.m;
-            uint32_t op = 0, rem = row;
-            if (epi.mode == kEpilogueConvert) {
-                op = row / epi.n;
-                rem = row - op * epi.n;
+            uint32_t op = 0, column = 0;
+            uint64_t out_row = 0;
+            if (row_ok) {
+                if (epi.mode == kEpilogueConvert)
+                    shape.rows.residue(row, op, column);
+                else
+                    out_row = shape.rows.row(row);
             }
             const uint32_t t_base = tmem + acc * kAccColumns + ((quarter * 32) << 16);
             for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 tmem_load32(t_base + chunk * 32, v);
                 if (!row_ok) continue;
                 if (epi.mode == kEpilogueRaw) {
-                    int32_t* out = epi.raw + size_t(row) * epi.raw_ld;
+                    int32_t* out = epi.raw + out_row * epi.raw_ld;
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         if (c_base + j < shape.columns) out[c_base + j] = int32_t(v[j]);
@@ -326,10 +329,10 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                     if (epi.mode == kEpilogueConvert) {
                         if (group_index < epi.r) {
                             const DevicePrime f = epi.primes[group_index];
-                            epi.residues[(size_t(op) * epi.r + group_index) * epi.n + rem] = redc(s, f.p, f.pinv);
+                            epi.residues[(size_t(op) * epi.r + group_index) * epi.n + column] = redc(s, f.p, f.pinv);
                         }
                     } else if (group_index < epi.words) {
-                        epi.dots[size_t(row) * epi.words + group_index] = s;
+                        epi.dots[out_row * epi.words + group_index] = s;
                     }
                 }
             }
@@ -397,10 +400,13 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     if (rows.mode == kRowsSplit) {
         split = rows.split;
         slab = rows.n_sub;
-        if (m != 2 * rows.n) {
-            why = "split row map expects both operands";
+        if (m != 2 * rows.n || rows.first != 0 || rows.span != rows.n_sub) {
+            why = "split row map expects both whole operands";
             return false;
         }
+    } else if (rows.first != 0) {
+        why = "linear row map must start at row 0";
+        return false;
     }
     if (slab < kBlockM || (rows.mode == kRowsSplit && slab % kBlockM)) {
         why = "fewer than 128 rows per transform";
@@ -441,6 +447,7 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     plan.n_tiles = (columns + kBlockN - 1) / kBlockN;
     plan.k_tiles = (k_bytes + kBlockK - 1) / kBlockK;
     plan.rows = rows;
+    plan.a_tile_bytes = uint64_t(kBlockM) * k_bytes;
     plan.error_flag = tensor_gemm_error_flag();
     int device = 0, sms = 0;
     cudaGetDevice(&device);
@@ -450,11 +457,28 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     return true;
 }
 
-void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {
-    TileShape shape{plan.m, plan.columns, plan.k_tiles, plan.m_tiles, plan.n_tiles, plan.rows};
-    const uint32_t tiles = plan.m_tiles * plan.n_tiles;
+bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_t m) {
+    if (!plan.ready || rows.mode != plan.rows.mode) return false;
+    if (rows.mode == kRowsSplit)
+        return rows.span % kBlockM == 0 && rows.first % kBlockM == 0 && rows.first + rows.span <= plan.rows.n_sub &&
+               m == 2 * rows.split * rows.span;
+    return uint64_t(rows.first) + m <= plan.m;
+}
+
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
+                        uint32_t m) {
+    const uint32_t m_tiles = (m + kBlockM - 1) / kBlockM;
+    // largest raster group whose A tiles fit comfortably in L2 (~48 MB)
+    uint64_t group = (48ull << 20) / plan.a_tile_bytes;
+    group = group < 8 ? 8 : (group > 64 ? 64 : group);
+    TileShape shape{m, plan.columns, plan.k_tiles, m_tiles, plan.n_tiles, uint32_t(group), rows};
+    const uint32_t tiles = m_tiles * plan.n_tiles;
     const uint32_t grid = tiles < plan.sm_count ? tiles : plan.sm_count;
     gemm_tc_kernel<<<grid, kThreads, kSmemBytes, stream>>>(plan.a_map, plan.b_map, shape, epilogue);
+}
+
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {
+    launch_gemm_tensor(plan, epilogue, stream, plan.rows, plan.m);
 }
 
 }  // namespace negacyclic

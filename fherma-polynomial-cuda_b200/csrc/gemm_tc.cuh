@@ -17,6 +17,7 @@ struct TensorGemmPlan {
     RowMap rows{};
     uint32_t* error_flag = nullptr;  // device word set when a pipeline wait times out
     uint32_t sm_count = 148;          // persistent grid size
+    uint64_t a_tile_bytes = 0;        // bytes of one 128-row A tile (raster group sizing)
     bool ready = false;
 };
 
@@ -26,6 +27,12 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
                          const uint8_t* b, uint32_t columns, uint32_t k_bytes, std::string& why);
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream);
+
+// A launch over part of the rows (a chunk of coefficients): `rows`/`m` describe the chunk
+// within the shape the plan was prepared for (see gemm_tensor_accepts).
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
+                        uint32_t m);
+bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_t m);
 
 // Device word that records pipeline-wait timeouts of the tensor GEMM (0 = none).
 uint32_t* tensor_gemm_error_flag();

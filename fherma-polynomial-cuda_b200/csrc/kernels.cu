@@ -133,10 +133,11 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restric
         uint32_t m = m0 + tr * 4 + i;
         if (m >= m_total) continue;
         if (epi.mode == kEpilogueRaw) {
+            const uint64_t out_row = rows.row(m);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 uint32_t c = c0 + tc * 4 + j;
-                if (c < columns) epi.raw[size_t(m) * epi.raw_ld + c] = int32_t(acc[i][j]);
+                if (c < columns) epi.raw[out_row * epi.raw_ld + c] = int32_t(acc[i][j]);
             }
             continue;
         }
@@ -145,10 +146,11 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restric
         if (epi.mode == kEpilogueConvert) {
             if (group >= epi.r) continue;
             const DevicePrime f = epi.primes[group];
-            uint32_t op = m / epi.n, rem = m - op * epi.n;
-            epi.residues[(size_t(op) * epi.r + group) * epi.n + rem] = redc(s, f.p, f.pinv);
+            uint32_t op, column;
+            rows.residue(m, op, column);
+            epi.residues[(size_t(op) * epi.r + group) * epi.n + column] = redc(s, f.p, f.pinv);
         } else {
-            if (group < epi.words) epi.dots[size_t(m) * epi.words + group] = s;
+            if (group < epi.words) epi.dots[rows.row(m) * epi.words + group] = s;
         }
     }
 }
@@ -257,34 +259,34 @@ __device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t base, 
     }
 }
 
-// One pass of R stages over all of this thread's groups. src/dst are shared
-// (padded index) or global (plain index); `scale` multiplies values stored to global.
-template <int R, bool kForward, bool kFromGlobal, bool kToGlobal>
-__device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, uint32_t log_t_min, uint32_t log_n,
-                                         const uint2* __restrict__ table, uint32_t p, bool scale, uint32_t f,
-                                         uint32_t f_q) {
+// One pass of R stages over all of this thread's groups (transform length 2^kLog,
+// 2^(kLog-4) threads). src/dst are shared (padded index) or global (plain index);
+// kScale multiplies the values stored to global by (f, f_q).
+template <int R, bool kForward, bool kFromGlobal, bool kToGlobal, bool kScale, uint32_t kLogTMin, uint32_t kLog>
+__device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, const uint2* __restrict__ table,
+                                         uint32_t p, uint32_t f, uint32_t f_q) {
     constexpr int G = kPerThread >> R;  // groups per thread
-    const uint32_t threads = blockDim.x;
+    constexpr uint32_t kThreads = 1u << (kLog - 4);
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-        const uint32_t group = threadIdx.x + g * threads;
-        const uint32_t off = group & ((1u << log_t_min) - 1);
-        const uint32_t base = ((group >> log_t_min) << (log_t_min + R)) + off;
+        const uint32_t group = threadIdx.x + g * kThreads;
+        const uint32_t off = group & ((1u << kLogTMin) - 1);
+        const uint32_t base = ((group >> kLogTMin) << (kLogTMin + R)) + off;
         uint32_t x[1 << R];
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
-            const uint32_t i = base + (uint32_t(k) << log_t_min);
+            const uint32_t i = base + (uint32_t(k) << kLogTMin);
             x[k] = kFromGlobal ? src[i] : src[padded(i)];
         }
         if (kForward)
-            ct_stages<R>(x, base, log_t_min, log_n, table, p);
+            ct_stages<R>(x, base, kLogTMin, kLog, table, p);
         else
-            gs_stages<R>(x, base, log_t_min, log_n, table, p);
+            gs_stages<R>(x, base, kLogTMin, kLog, table, p);
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
-            const uint32_t i = base + (uint32_t(k) << log_t_min);
+            const uint32_t i = base + (uint32_t(k) << kLogTMin);
             uint32_t value = x[k];
-            if (kToGlobal && scale) value = shoup(value, f, f_q, p);
+            if (kScale) value = shoup(value, f, f_q, p);
             if (kToGlobal)
                 dst[i] = value;
             else
@@ -293,61 +295,44 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, uin
     }
 }
 
-template <bool kForward, bool kFromGlobal, bool kToGlobal>
-__device__ __forceinline__ void ntt_pass_r(int R, const uint32_t* src, uint32_t* dst, uint32_t log_t_min,
-                                           uint32_t log_n, const uint2* __restrict__ table, uint32_t p, bool scale,
+// Passes kDone.. of a length-2^kLog transform: four stages per pass, the remainder last.
+// Forward runs half-sizes large -> small; inverse small -> large and scales its output.
+template <bool kForward, uint32_t kLog, uint32_t kDone>
+__device__ __forceinline__ void ntt_passes(uint32_t* data, uint32_t* xs, const uint2* __restrict__ table, uint32_t p,
                                            uint32_t f, uint32_t f_q) {
-    switch (R) {
-        case 4: ntt_pass<4, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
-        case 3: ntt_pass<3, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
-        case 2: ntt_pass<2, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
-        default: ntt_pass<1, kForward, kFromGlobal, kToGlobal>(src, dst, log_t_min, log_n, table, p, scale, f, f_q); break;
+    constexpr int R = (kLog - kDone) < 4 ? int(kLog - kDone) : 4;
+    constexpr uint32_t kLogTMin = kForward ? kLog - kDone - R : kDone;
+    constexpr bool kFirst = kDone == 0, kLast = kDone + R == kLog;
+    ntt_pass<R, kForward, kFirst, kLast, kLast && !kForward, kLogTMin, kLog>(kFirst ? data : xs, kLast ? data : xs,
+                                                                              table, p, f, f_q);
+    if constexpr (!kLast) {
+        __syncthreads();
+        ntt_passes<kForward, kLog, kDone + R>(data, xs, table, p, f, f_q);
     }
 }
 
-// Whole transform of `data` (length 2^log_n, log_n >= 8) in place: passes of four
-// stages, then the remainder; forward runs half-sizes large -> small, inverse
-// small -> large and multiplies its output by (f, f_q).
-template <bool kForward>
-__device__ __forceinline__ void ntt_blocked(uint32_t* data, uint32_t* xs, uint32_t log_n, const uint2* table,
-                                            uint32_t p, uint32_t f, uint32_t f_q) {
-    const uint32_t passes = (log_n + 3) / 4;
-    uint32_t done = 0;
-    for (uint32_t pass = 0; pass < passes; ++pass) {
-        const int R = int(min(4u, log_n - done));
-        // forward: the pass's smallest half-size is n / 2^(done + R); inverse: 2^done
-        const uint32_t log_t_min = kForward ? log_n - done - R : done;
-        const bool first = pass == 0, last = pass + 1 == passes;
-        if (first)
-            ntt_pass_r<kForward, true, false>(R, data, xs, log_t_min, log_n, table, p, false, f, f_q);
-        else if (last)
-            ntt_pass_r<kForward, false, true>(R, xs, data, log_t_min, log_n, table, p, !kForward, f, f_q);
-        else
-            ntt_pass_r<kForward, false, false>(R, xs, xs, log_t_min, log_n, table, p, false, f, f_q);
-        done += R;
-        if (!last) __syncthreads();
-    }
+// grid (2s, r): x = op*s + t, y = prime, so a prime's 2s transforms share its twiddles in L2
+template <uint32_t kLog>
+__global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_forward_blocked_kernel(
+    uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
+    uint32_t split) {
+    extern __shared__ uint32_t xs[];
+    constexpr uint32_t kN = 1u << kLog;
+    const uint32_t op = blockIdx.x / split, t_index = blockIdx.x - op * split, k = blockIdx.y;
+    uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * kN;
+    ntt_passes<true, kLog, 0>(data, xs, fwd + size_t(k) * kN, primes[k].p, 0, 0);
 }
 
-__global__ void __launch_bounds__(512) ntt_forward_blocked_kernel(uint32_t* residues,
-                                                                  const DevicePrime* __restrict__ primes,
-                                                                  const uint2* __restrict__ fwd, uint32_t r,
-                                                                  uint32_t n, uint32_t n_sub, uint32_t log_n) {
+template <uint32_t kLog>
+__global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_inverse_blocked_kernel(
+    uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ inv, uint32_t r, uint32_t n,
+    uint32_t split) {
     extern __shared__ uint32_t xs[];
-    const uint32_t t_index = blockIdx.x, k = blockIdx.y, op = blockIdx.z;
-    uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * n_sub;
-    ntt_blocked<true>(data, xs, log_n, fwd + size_t(k) * n_sub, primes[k].p, 0, 0);
-}
-
-__global__ void __launch_bounds__(512) ntt_inverse_blocked_kernel(uint32_t* residues,
-                                                                  const DevicePrime* __restrict__ primes,
-                                                                  const uint2* __restrict__ inv, uint32_t r,
-                                                                  uint32_t n, uint32_t n_sub, uint32_t log_n) {
-    extern __shared__ uint32_t xs[];
+    constexpr uint32_t kN = 1u << kLog;
     const uint32_t v_index = blockIdx.x, k = blockIdx.y;
     const DevicePrime f = primes[k];
-    uint32_t* data = residues + size_t(k) * n + size_t(v_index) * n_sub;
-    ntt_blocked<false>(data, xs, log_n, inv + size_t(k) * n_sub, f.p, f.finish, f.finish_q);
+    uint32_t* data = residues + size_t(k) * n + size_t(v_index) * kN;
+    ntt_passes<false, kLog, 0>(data, xs, inv + size_t(k) * kN, f.p, f.finish, f.finish_q);
 }
 
 // C_v = sum_{t+u=v} A_t B_u + zeta * sum_{t+u=v+s} A_t B_u at every evaluation point,
@@ -368,13 +353,22 @@ __global__ void pointwise_kernel(uint32_t* residues, const DevicePrime* __restri
         bv[t] = b[size_t(t) * n_sub];
     }
     const uint2 z = zeta[size_t(k) * n_sub + m];
+    // two products per Montgomery reduction: a b + a' b' < 2 p^2 < p 2^32
 #pragma unroll
     for (int v = 0; v < S; ++v) {
         uint32_t low = 0, wrap = 0;
 #pragma unroll
-        for (int t = 0; t <= v; ++t) low = add_mod(low, mont(av[t], bv[v - t], f.p, f.pinv), f.p);
+        for (int t = 0; t <= v; t += 2) {
+            uint64_t pair = uint64_t(av[t]) * bv[v - t];
+            if (t + 1 <= v) pair += uint64_t(av[t + 1]) * bv[v - t - 1];
+            low = add_mod(low, redc(pair, f.p, f.pinv), f.p);
+        }
 #pragma unroll
-        for (int t = v + 1; t < S; ++t) wrap = add_mod(wrap, mont(av[t], bv[v + S - t], f.p, f.pinv), f.p);
+        for (int t = v + 1; t < S; t += 2) {
+            uint64_t pair = uint64_t(av[t]) * bv[v + S - t];
+            if (t + 1 < S) pair += uint64_t(av[t + 1]) * bv[v + S - t - 1];
+            wrap = add_mod(wrap, redc(pair, f.p, f.pinv), f.p);
+        }
         a[size_t(v) * n_sub] = add_mod(low, shoup(wrap, z.x, z.y, f.p), f.p);
     }
 }
@@ -474,61 +468,82 @@ __device__ __forceinline__ int compare_q(const uint32_t* v, uint32_t len, const 
 }
 
 // One warp per coefficient; its words live in shared memory.
+//
+// The CRT word sums split cleanly: words [0, L+2) are a carry-save form of
+// T = sum v_k M_k (< 2^(32(L+2)), so nothing carries out of them), words
+// L+2..L+4 a carry-save form of D = sum v_k floor(2^64/p_k). Hence
+//   K  = (D + 2^63) >> 64 straight from three word sums,
+//   T' = T + K*(-P mod q) in one carry pass over dots[w] + K*R[w],
+//   c  = T' - quotient*q in one signed carry pass, then at most three q's off.
 __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
     extern __shared__ uint32_t scratch[];
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x & 31;
     const uint32_t warps = blockDim.x / 32;
     uint32_t* v = scratch + size_t(warp) * stride;
     const uint32_t words = prm.words, limbs = prm.limbs, tlen = limbs + 2;
+    const uint32_t* q = prm.q;
     for (uint32_t i = blockIdx.x * warps + warp; i < prm.n; i += gridDim.x * warps) {
-        // 1. carry-save word sums -> exact words V (V < 2^(32 words))
         const uint64_t* d = prm.dots + size_t(i) * words;
+        // 1. K = (D + 2^63) >> 64, D = d[L+2] + d[L+3] 2^32 + d[L+4] 2^64 (each word sum < 2^56)
+        const uint64_t x0 = d[limbs + 2], x1 = d[limbs + 3], x2 = d[limbs + 4];
+        const uint64_t low = x0 + (x1 << 32);
+        const uint64_t high = (x1 >> 32) + x2 + (low < x0 ? 1 : 0);  // D = high 2^64 + low
+        const uint64_t kq = high + ((low + (1ull << 63)) < low ? 1 : 0);
+        // 2. T' = sum_w (d[w] + K R[w]) 2^(32w), collapsed to exact words in one carry pass
         uint32_t chain = 0, carried_high = 0;
-        for (uint32_t base = 0; base <= words; base += 32) {
-            uint32_t w = base + lane;
-            uint64_t value = w < words ? d[w] : 0ull;
-            uint32_t high = uint32_t(value >> 32);
-            uint32_t below = __shfl_up_sync(kFull, high, 1);
+        for (uint32_t base = 0; base < tlen; base += 32) {
+            const uint32_t w = base + lane;
+            uint64_t value = 0;
+            if (w < tlen) value = d[w] + (w < limbs ? kq * prm.minus_p[w] : 0ull);
+            const uint32_t high32 = uint32_t(value >> 32);
+            uint32_t below = __shfl_up_sync(kFull, high32, 1);
             if (lane == 0) below = carried_high;
-            carried_high = __shfl_sync(kFull, high, 31);
-            uint64_t sum = uint64_t(uint32_t(value)) + below;
-            uint32_t low = uint32_t(sum);
-            uint32_t carry = chain_carry((sum >> 32) != 0, low == kFull, chain);
-            if (w < stride) v[w] = low + carry;
+            carried_high = __shfl_sync(kFull, high32, 31);
+            const uint64_t sum = uint64_t(uint32_t(value)) + below;
+            const uint32_t word = uint32_t(sum);
+            const uint32_t carry = chain_carry((sum >> 32) != 0, word == kFull, chain);
+            if (w < tlen) v[w] = word + carry;
         }
         __syncwarp();
-        // 2. CRT quotient K = (D + 2^63) >> 64, D = V >> 32(L+2)
-        const uint32_t kq = v[limbs + 4] + (v[limbs + 3] >> 31);
-        // 3. T' = T + K * (-P mod q), T = V mod 2^(32(L+2))
-        add_words(v, tlen, [&](uint32_t w) { return w < limbs ? uint32_t(uint64_t(kq) * prm.minus_p[w]) : 0u; });
-        add_words(v, tlen, [&](uint32_t w) {
-            return (w >= 1 && w - 1 < limbs) ? uint32_t((uint64_t(kq) * prm.minus_p[w - 1]) >> 32) : 0u;
-        });
-        // 4. Barrett quotient from the 128 bits of T' at q's top-64-bit window
-        uint64_t tl = uint64_t(bits_word(v, prm.top_shift, tlen)) |
-                      (uint64_t(bits_word(v, int64_t(prm.top_shift) + 32, tlen)) << 32);
-        uint64_t th = uint64_t(bits_word(v, int64_t(prm.top_shift) + 64, tlen)) |
-                      (uint64_t(bits_word(v, int64_t(prm.top_shift) + 96, tlen)) << 32);
-        uint64_t prod_l_hi = __umul64hi(tl, prm.mu_low);
-        uint64_t prod_h_lo = th * prm.mu_low, prod_h_hi = __umul64hi(th, prm.mu_low);
-        uint64_t word1 = prod_l_hi + prod_h_lo;
-        uint64_t word2 = prod_h_hi + (word1 < prod_l_hi ? 1 : 0);
-        uint64_t c2 = (tl + word1 < tl) ? 1 : 0;
-        const uint64_t quotient = th + word2 + c2;
+        // 3. Barrett quotient from the 128 bits of T' at q's top-64-bit window
+        const uint64_t tl = uint64_t(bits_word(v, prm.top_shift, tlen)) |
+                            (uint64_t(bits_word(v, int64_t(prm.top_shift) + 32, tlen)) << 32);
+        const uint64_t th = uint64_t(bits_word(v, int64_t(prm.top_shift) + 64, tlen)) |
+                            (uint64_t(bits_word(v, int64_t(prm.top_shift) + 96, tlen)) << 32);
+        const uint64_t prod_l_hi = __umul64hi(tl, prm.mu_low);
+        const uint64_t prod_h_lo = th * prm.mu_low, prod_h_hi = __umul64hi(th, prm.mu_low);
+        const uint64_t word1 = prod_l_hi + prod_h_lo;
+        const uint64_t word2 = prod_h_hi + (word1 < prod_l_hi ? 1 : 0);
+        const uint64_t quotient = th + word2 + ((tl + word1 < tl) ? 1 : 0);
         const uint32_t ql = uint32_t(quotient), qh = uint32_t(quotient >> 32);
-        // 5. T' -= quotient * q, as four word streams
-        const uint32_t* q = prm.q;
-        sub_words(v, tlen, [&](uint32_t w) { return w < limbs ? uint32_t(uint64_t(ql) * q[w]) : 0u; });
-        sub_words(v, tlen, [&](uint32_t w) {
-            return (w >= 1 && w - 1 < limbs) ? uint32_t((uint64_t(ql) * q[w - 1]) >> 32) : 0u;
-        });
-        sub_words(v, tlen, [&](uint32_t w) {
-            return (w >= 1 && w - 1 < limbs) ? uint32_t(uint64_t(qh) * q[w - 1]) : 0u;
-        });
-        sub_words(v, tlen, [&](uint32_t w) {
-            return (w >= 2 && w - 2 < limbs) ? uint32_t((uint64_t(qh) * q[w - 2]) >> 32) : 0u;
-        });
-        // 6. at most three subtractions of q remain
+        __syncwarp();
+        // 4. c = T' - quotient*q in one signed carry pass. With a_w = ql q[w], b_w = qh q[w-1]:
+        //    z_w = T'[w] - lo(a_w) - lo(b_w) - hi(a_{w-1}) - hi(b_{w-1})  in (-2^35, 2^32)
+        chain = 0;
+        uint64_t carry_hi = 0;  // hi(a)+hi(b) of the previous chunk's last lane
+        int32_t carry_c = 0;    // signed word carry of the previous chunk's last lane
+        for (uint32_t base = 0; base < tlen; base += 32) {
+            const uint32_t w = base + lane;
+            const uint32_t qw = w < limbs ? q[w] : 0u;
+            const uint32_t qw1 = (w >= 1 && w - 1 < limbs) ? q[w - 1] : 0u;
+            const uint64_t a = uint64_t(ql) * qw, b = uint64_t(qh) * qw1;
+            const uint64_t hi = (a >> 32) + (b >> 32);
+            uint64_t hi_below = (uint64_t(__shfl_up_sync(kFull, uint32_t(hi >> 32), 1)) << 32) |
+                                __shfl_up_sync(kFull, uint32_t(hi), 1);
+            if (lane == 0) hi_below = carry_hi;
+            carry_hi = (uint64_t(__shfl_sync(kFull, uint32_t(hi >> 32), 31)) << 32) | __shfl_sync(kFull, uint32_t(hi), 31);
+            const uint64_t e = (a & 0xffffffffull) + (b & 0xffffffffull) + hi_below;
+            const int64_t z = int64_t(w < tlen ? v[w] : 0u) - int64_t(e);
+            const int32_t c = int32_t(z >> 32);  // floor(z / 2^32), in [-8, 0]
+            int32_t c_below = __shfl_up_sync(kFull, c, 1);
+            if (lane == 0) c_below = carry_c;
+            carry_c = __shfl_sync(kFull, c, 31);
+            const int64_t sw = int64_t(uint32_t(z)) + c_below;  // in [-8, 2^32)
+            const uint32_t borrow = chain_carry(sw < 0, sw == 0, chain);
+            if (w < tlen) v[w] = uint32_t(sw - borrow);
+        }
+        __syncwarp();
+        // 5. at most three subtractions of q remain
         int corrections = 0;
         while (compare_q(v, tlen, q, limbs) >= 0) {
             if (++corrections > 3) {
@@ -537,12 +552,13 @@ __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
             }
             sub_words(v, tlen, [&](uint32_t w) { return w < limbs ? q[w] : 0u; });
         }
-        // 7. canonical result
+        // 6. canonical result
         uint32_t* out = prm.out + size_t(i) * limbs;
         for (uint32_t w = lane; w < limbs; w += 32) out[w] = v[w];
         __syncwarp();
     }
 }
+
 
 uint32_t log2_u32(uint32_t x) { return x ? 31 - __builtin_clz(x) : 0; }
 
@@ -584,28 +600,47 @@ static uint32_t ntt_threads(uint32_t n_sub) {
     return half >= 512 ? 512 : (half >= 32 ? half : 32);
 }
 
+template <bool kForward, uint32_t kLog>
+static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const uint2* table, uint32_t r, uint32_t n,
+                           uint32_t split, cudaStream_t stream) {
+    constexpr uint32_t kN = 1u << kLog;
+    const size_t smem = (kN + kN / 32) * sizeof(uint32_t);
+    auto kernel = kForward ? ntt_forward_blocked_kernel<kLog> : ntt_inverse_blocked_kernel<kLog>;
+    static bool configured = false;
+    if (!configured) {  // room for several transforms per SM
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        configured = true;
+    }
+    dim3 grid(kForward ? 2 * split : split, r);
+    kernel<<<grid, kN / kPerThread, smem, stream>>>(residues, primes, table, r, n, split);
+}
+
+template <bool kForward>
+static bool launch_blocked_any(uint32_t n_sub, uint32_t* residues, const DevicePrime* primes, const uint2* table,
+                               uint32_t r, uint32_t n, uint32_t split, cudaStream_t stream) {
+    switch (n_sub) {
+        case 256: launch_blocked<kForward, 8>(residues, primes, table, r, n, split, stream); return true;
+        case 512: launch_blocked<kForward, 9>(residues, primes, table, r, n, split, stream); return true;
+        case 1024: launch_blocked<kForward, 10>(residues, primes, table, r, n, split, stream); return true;
+        case 2048: launch_blocked<kForward, 11>(residues, primes, table, r, n, split, stream); return true;
+        case 4096: launch_blocked<kForward, 12>(residues, primes, table, r, n, split, stream); return true;
+        case 8192: launch_blocked<kForward, 13>(residues, primes, table, r, n, split, stream); return true;
+        default: return false;
+    }
+}
+
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r, uint32_t n,
                         uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    if (launch_blocked_any<true>(n_sub, residues, primes, fwd, r, n, split, stream)) return;
     dim3 grid(split, r, 2);
-    if (n_sub >= 256) {
-        const size_t smem = (n_sub + n_sub / 32) * sizeof(uint32_t);
-        ntt_forward_blocked_kernel<<<grid, n_sub / kPerThread, smem, stream>>>(residues, primes, fwd, r, n, n_sub,
-                                                                                log2_u32(n_sub));
-        return;
-    }
     ntt_forward_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, fwd, r, n,
                                                                                           n_sub);
 }
 
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r, uint32_t n,
                         uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    if (launch_blocked_any<false>(n_sub, residues, primes, inv, r, n, split, stream)) return;
     dim3 grid(split, r);
-    if (n_sub >= 256) {
-        const size_t smem = (n_sub + n_sub / 32) * sizeof(uint32_t);
-        ntt_inverse_blocked_kernel<<<grid, n_sub / kPerThread, smem, stream>>>(residues, primes, inv, r, n, n_sub,
-                                                                                log2_u32(n_sub));
-        return;
-    }
     ntt_inverse_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, inv, r, n,
                                                                                           n_sub);
 }

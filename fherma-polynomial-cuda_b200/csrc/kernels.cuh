@@ -7,20 +7,42 @@
 
 namespace negacyclic {
 
-// Row addressing of the u8 GEMM's A operand.
-//  kRowsLinear:   row m at base + m * pitch
-//  kRowsSplit:    row rho = op*N + t*N' + j reads coefficient i = s*j + t of operand op
-//                 from base + (op*N + i) * pitch  (conversion of the split ring)
+// Row addressing of the u8 GEMM's A operand, for one launch (a whole product or a chunk).
+//  kRowsLinear: GEMM row m reads operand row first + m.
+//  kRowsSplit:  GEMM row m = op*(s*span) + t*span + (j - first), j in [first, first+span),
+//               reads coefficient i = s*j + t of operand op (operand row op*N + i) and
+//               produces residue row op, column t*N' + j (transform t, position j).
 enum RowMode : int { kRowsLinear = 0, kRowsSplit = 1 };
 
 struct RowMap {
     int mode;
     uint32_t n, n_sub, split;
+    uint32_t first;  // linear: first operand row; split: first j
+    uint32_t span;   // split: j values per (operand, t) in this launch
+
+    static RowMap linear(uint32_t first_row) { return RowMap{kRowsLinear, 0, 0, 1, first_row, 0}; }
+    static RowMap split_rows(uint32_t n, uint32_t n_sub, uint32_t split, uint32_t first_j, uint32_t j_span) {
+        return RowMap{kRowsSplit, n, n_sub, split, first_j, j_span};
+    }
+    __host__ __device__ __forceinline__ void decompose(uint32_t m, uint32_t& op, uint32_t& t, uint32_t& j) const {
+        const uint32_t per_op = split * span;
+        op = m / per_op;
+        const uint32_t rem = m - op * per_op;
+        t = rem / span;
+        j = first + (rem - t * span);
+    }
+    // operand row read by GEMM row m
     __device__ __forceinline__ uint64_t row(uint32_t m) const {
-        if (mode == kRowsLinear) return m;
-        uint32_t op = m / n, rem = m - op * n;
-        uint32_t t = rem / n_sub, j = rem - t * n_sub;
+        if (mode == kRowsLinear) return uint64_t(first) + m;
+        uint32_t op, t, j;
+        decompose(m, op, t, j);
         return uint64_t(op) * n + uint64_t(j) * split + t;
+    }
+    // conversion output position of GEMM row m: residue row `op`, column t*N' + j
+    __device__ __forceinline__ void residue(uint32_t m, uint32_t& op, uint32_t& column) const {
+        uint32_t t, j;
+        decompose(m, op, t, j);
+        column = t * n_sub + j;
     }
 };
 
@@ -30,14 +52,14 @@ enum EpilogueMode : int { kEpilogueRaw = 0, kEpilogueConvert = 1, kEpilogueCrt =
 
 struct Epilogue {
     int mode;
-    // raw: D[m][col] int32, ld = columns
+    // raw: D[row][col] int32, ld = columns, row = the operand row of GEMM row m
     int32_t* raw;
     uint32_t raw_ld;
-    // convert: residues[(op*r + k)*N + rem] = redc(S, p_k), for m = op*N + rem, g = k < r
+    // convert: residues[(op*r + k)*N + column] = redc(S, p_k), (op, column) = RowMap::residue(m), g = k < r
     uint32_t* residues;
     const DevicePrime* primes;
     uint32_t r, n;
-    // crt: dots[m * words + g] = S (u64), g < words
+    // crt: dots[row * words + g] = S (u64), g < words, row = the operand row of GEMM row m
     uint64_t* dots;
     uint32_t words;
 };

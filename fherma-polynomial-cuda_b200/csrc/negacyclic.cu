@@ -64,7 +64,10 @@ struct negacyclic_plan {
     uint32_t *operands = nullptr, *residues = nullptr, *crt_in = nullptr, *result = nullptr;
     uint64_t* dots = nullptr;
     uint32_t* error_flag = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
+    static constexpr uint32_t kMaxChunks = 16;
+    uint32_t chunks = 1;  // coefficient chunks of the streamed host path
+    cudaEvent_t in_ready[kMaxChunks] = {}, out_ready[kMaxChunks] = {};
     size_t device_bytes = 0, table_bytes = 0;
     TensorGemmPlan convert_gemm, crt_gemm;
 
@@ -77,7 +80,15 @@ struct negacyclic_plan {
                            operands, residues, crt_in, result, dots, error_flag};
         for (void* ptr : buffers)
             if (ptr) cudaFree(ptr);
+        if (copy_in) cudaStreamSynchronize(copy_in);
+        if (copy_out) cudaStreamSynchronize(copy_out);
+        for (uint32_t c = 0; c < kMaxChunks; ++c) {
+            if (in_ready[c]) cudaEventDestroy(in_ready[c]);
+            if (out_ready[c]) cudaEventDestroy(out_ready[c]);
+        }
         if (stream) cudaStreamDestroy(stream);
+        if (copy_in) cudaStreamDestroy(copy_in);
+        if (copy_out) cudaStreamDestroy(copy_out);
         cudaSetDevice(previous);
     }
 };
@@ -86,9 +97,55 @@ namespace {
 
 constexpr uint32_t kStages = 7;  // convert, forward, pointwise, inverse, transpose, crt, reduce
 
-// Enqueues the whole product on `stream`. `operands` already holds the padded inputs.
-// `marks` (optional, kStages events) are recorded after each stage.
-void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cudaEvent_t* marks = nullptr) {
+// conversion GEMM over the coefficients s*j + t, j in [first_j, first_j + span), all t, both operands
+void enqueue_convert(negacyclic_plan& s, uint32_t first_j, uint32_t span, cudaStream_t stream) {
+    const HostPlan& h = s.host;
+    Epilogue convert{};
+    convert.mode = kEpilogueConvert;
+    convert.residues = s.residues;
+    convert.primes = s.primes;
+    convert.r = s.r;
+    convert.n = h.n;
+    const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span);
+    const uint32_t m = 2 * h.split * span;
+    if (s.convert_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.convert_gemm, rows, m))
+        launch_gemm_tensor(s.convert_gemm, convert, stream, rows, m);
+    else
+        launch_gemm_simt(reinterpret_cast<const uint8_t*>(s.operands), uint64_t(s.padded_limbs) * 4, rows, m,
+                         s.convert_weights, 4 * s.padded_r, s.k_convert, convert, stream);
+}
+
+// CRT GEMM and reduction of coefficients [first, first + count) into d_c (rows indexed from 0 = coefficient 0)
+void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t* d_c, cudaStream_t stream,
+                    cudaEvent_t between = nullptr) {
+    const HostPlan& h = s.host;
+    Epilogue crt{};
+    crt.mode = kEpilogueCrt;
+    crt.dots = s.dots;
+    crt.words = h.words;
+    const RowMap rows = RowMap::linear(first);
+    if (s.crt_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.crt_gemm, rows, count))
+        launch_gemm_tensor(s.crt_gemm, crt, stream, rows, count);
+    else
+        launch_gemm_simt(reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4, rows, count,
+                         s.crt_weights, s.crt_columns, s.k_crt, crt, stream);
+    if (between) check(cudaEventRecord(between, stream), "cudaEventRecord");
+    ReduceParams reduce{};
+    reduce.dots = s.dots + size_t(first) * h.words;
+    reduce.out = d_c + size_t(first) * h.limbs;
+    reduce.q = s.q;
+    reduce.minus_p = s.minus_p;
+    reduce.n = count;
+    reduce.limbs = h.limbs;
+    reduce.words = h.words;
+    reduce.top_shift = h.top_shift;
+    reduce.mu_low = h.mu_low;
+    reduce.error_flag = s.error_flag;
+    launch_reduce(reduce, stream);
+}
+
+// forward NTTs, pointwise products, inverse NTTs, transpose
+void enqueue_middle(negacyclic_plan& s, cudaStream_t stream, cudaEvent_t* marks) {
     const HostPlan& h = s.host;
     const uint32_t n = h.n;
     uint32_t stage = 0;
@@ -96,21 +153,6 @@ void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cud
         if (marks) check(cudaEventRecord(marks[stage], stream), "cudaEventRecord");
         ++stage;
     };
-    // convert: rows rho = op*N + t*N' + j  (coefficient s*j + t of operand op)
-    Epilogue convert{};
-    convert.mode = kEpilogueConvert;
-    convert.residues = s.residues;
-    convert.primes = s.primes;
-    convert.r = s.r;
-    convert.n = n;
-    if (s.convert_engine == NEGACYCLIC_GEMM_TENSOR) {
-        launch_gemm_tensor(s.convert_gemm, convert, stream);
-    } else {
-        RowMap rows{kRowsSplit, n, h.n_sub, h.split};
-        launch_gemm_simt(reinterpret_cast<const uint8_t*>(s.operands), uint64_t(s.padded_limbs) * 4, rows, 2 * n,
-                         s.convert_weights, 4 * s.padded_r, s.k_convert, convert, stream);
-    }
-    mark();
     launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, n, h.n_sub, h.split, stream);
     mark();
     launch_pointwise(s.residues, s.primes, s.zeta, s.r, n, h.n_sub, h.split, stream);
@@ -119,31 +161,17 @@ void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cud
     mark();
     launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, n, h.n_sub, h.split, stream);
     mark();
-    Epilogue crt{};
-    crt.mode = kEpilogueCrt;
-    crt.dots = s.dots;
-    crt.words = h.words;
-    if (s.crt_engine == NEGACYCLIC_GEMM_TENSOR) {
-        launch_gemm_tensor(s.crt_gemm, crt, stream);
-    } else {
-        RowMap rows{kRowsLinear, n, h.n_sub, h.split};
-        launch_gemm_simt(reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4, rows, n, s.crt_weights,
-                         s.crt_columns, s.k_crt, crt, stream);
-    }
-    mark();
-    ReduceParams reduce{};
-    reduce.dots = s.dots;
-    reduce.out = d_c;
-    reduce.q = s.q;
-    reduce.minus_p = s.minus_p;
-    reduce.n = n;
-    reduce.limbs = h.limbs;
-    reduce.words = h.words;
-    reduce.top_shift = h.top_shift;
-    reduce.mu_low = h.mu_low;
-    reduce.error_flag = s.error_flag;
-    launch_reduce(reduce, stream);
-    mark();
+}
+
+// Enqueues the whole product on `stream`. `operands` already holds the padded inputs.
+// `marks` (optional, kStages events) are recorded after each stage.
+void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cudaEvent_t* marks = nullptr) {
+    const HostPlan& h = s.host;
+    enqueue_convert(s, 0, h.n_sub, stream);
+    if (marks) check(cudaEventRecord(marks[0], stream), "cudaEventRecord");
+    enqueue_middle(s, stream, marks ? marks + 1 : nullptr);
+    enqueue_output(s, 0, h.n, d_c, stream, marks ? marks[5] : nullptr);
+    if (marks) check(cudaEventRecord(marks[6], stream), "cudaEventRecord");
     check(cudaGetLastError(), "product kernels");
 }
 
@@ -225,6 +253,14 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
     s.crt_columns = round_up(4 * h.words, 64);
     try {
         check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&s.copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&s.copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
+        // host products stream in 8 coefficient chunks once each chunk keeps 128-row GEMM tiles
+        s.chunks = (h.n_sub >= 1024 && h.n >= 8192) ? 8 : 1;
+        for (uint32_t c = 0; c < s.chunks; ++c) {
+            check(cudaEventCreateWithFlags(&s.in_ready[c], cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&s.out_ready[c], cudaEventDisableTiming), "cudaEventCreate");
+        }
         size_t tables = 0, work = 0;
         device_alloc(s.primes, s.r, tables);
         device_alloc(s.fwd, size_t(s.r) * h.n_sub, tables);
@@ -267,11 +303,11 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         if (o.gemm != NEGACYCLIC_GEMM_SIMT) {
             std::string why_convert, why_crt;
             if (prepare_gemm_tensor(s.convert_gemm, reinterpret_cast<const uint8_t*>(s.operands),
-                                    uint64_t(s.padded_limbs) * 4, RowMap{kRowsSplit, n, h.n_sub, h.split}, 2 * n,
+                                    uint64_t(s.padded_limbs) * 4, RowMap::split_rows(n, h.n_sub, h.split, 0, h.n_sub), 2 * n,
                                     s.convert_weights, 4 * s.padded_r, s.k_convert, why_convert))
                 s.convert_engine = NEGACYCLIC_GEMM_TENSOR;
             if (prepare_gemm_tensor(s.crt_gemm, reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4,
-                                    RowMap{kRowsLinear, n, h.n_sub, h.split}, n, s.crt_weights, s.crt_columns,
+                                    RowMap::linear(0), n, s.crt_weights, s.crt_columns,
                                     s.k_crt, why_crt))
                 s.crt_engine = NEGACYCLIC_GEMM_TENSOR;
             if (o.gemm == NEGACYCLIC_GEMM_TENSOR &&
@@ -351,19 +387,44 @@ int negacyclic_run(negacyclic_plan* s, const uint32_t* a, const uint32_t* b, uin
     DeviceGuard guard(s->device);
     const HostPlan& h = s->host;
     const size_t row = size_t(h.limbs) * 4, pitch = size_t(s->padded_limbs) * 4;
+    const uint32_t chunks = s->chunks, per = h.n / chunks, span = h.n_sub / chunks;
     cudaStream_t st = s->stream;
     try {
-        // operands land directly in the padded layout (2-D copies skip the pad kernel)
-        check(cudaMemcpy2DAsync(s->operands, pitch, a, row, row, h.n, cudaMemcpyHostToDevice, st), "copy a");
-        check(cudaMemcpy2DAsync(s->operands + size_t(h.n) * s->padded_limbs, pitch, b, row, row, h.n,
-                                cudaMemcpyHostToDevice, st),
-              "copy b");
-        enqueue_product(*s, s->result, st);
-        check(cudaMemcpyAsync(c, s->result, size_t(h.n) * row, cudaMemcpyDeviceToHost, st), "copy c");
+        // inputs: chunk c's rows of a and b land in the padded operand layout (2-D copies, no pad
+        // kernel), then the conversion GEMM of that chunk runs while the next chunk is in flight
+        for (uint32_t k = 0; k < chunks; ++k) {
+            const size_t first = size_t(k) * per;
+            check(cudaMemcpy2DAsync(s->operands + first * s->padded_limbs, pitch, a + first * h.limbs, row, row, per,
+                                    cudaMemcpyHostToDevice, s->copy_in),
+                  "copy a");
+            check(cudaMemcpy2DAsync(s->operands + (size_t(h.n) + first) * s->padded_limbs, pitch,
+                                    b + first * h.limbs, row, row, per, cudaMemcpyHostToDevice, s->copy_in),
+                  "copy b");
+            check(cudaEventRecord(s->in_ready[k], s->copy_in), "cudaEventRecord");
+            check(cudaStreamWaitEvent(st, s->in_ready[k], 0), "cudaStreamWaitEvent");
+            enqueue_convert(*s, k * span, span, st);
+        }
+        enqueue_middle(*s, st, nullptr);
+        // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
+        for (uint32_t k = 0; k <= chunks; ++k) {
+            if (k < chunks) {
+                enqueue_output(*s, k * per, per, s->result, st);
+                check(cudaEventRecord(s->out_ready[k], st), "cudaEventRecord");
+            }
+            if (k >= 1) {
+                const size_t first = size_t(k - 1) * per;
+                check(cudaStreamWaitEvent(s->copy_out, s->out_ready[k - 1], 0), "cudaStreamWaitEvent");
+                check(cudaMemcpyAsync(c + first * h.limbs, s->result + first * h.limbs, size_t(per) * row,
+                                      cudaMemcpyDeviceToHost, s->copy_out),
+                      "copy c");
+            }
+        }
+        check(cudaGetLastError(), "product kernels");
         uint32_t flag = 0, pipeline = 0;
-        check(cudaMemcpyAsync(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost, st), "error flag");
+        check(cudaMemcpyAsync(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost, s->copy_out), "error flag");
         if (uint32_t* tc = tensor_gemm_error_flag())
-            check(cudaMemcpyAsync(&pipeline, tc, 4, cudaMemcpyDeviceToHost, st), "error flag");
+            check(cudaMemcpyAsync(&pipeline, tc, 4, cudaMemcpyDeviceToHost, s->copy_out), "error flag");
+        check(cudaStreamSynchronize(s->copy_out), "product");
         check(cudaStreamSynchronize(st), "product");
         if (flag) return fail(NEGACYCLIC_ECUDA, "reduction exceeded its proven correction bound");
         if (pipeline) return fail(NEGACYCLIC_ECUDA, "tensor-core GEMM pipeline wait timed out");
@@ -406,7 +467,7 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
     raw.mode = kEpilogueRaw;
     raw.raw = d_d;
     raw.raw_ld = n;
-    RowMap rows{kRowsLinear, m, m, 1};
+    RowMap rows = RowMap::linear(0);
     try {
         if (engine == NEGACYCLIC_GEMM_TENSOR) {
             TensorGemmPlan plan;
