@@ -25,7 +25,7 @@ LIBRARY = os.path.join(HERE, "libnegacyclic.so")
 SHIM_LIBRARY = os.path.join(HERE, "libfherma_negacyclic.so")
 
 OK, EINVAL, ENOFIELDS, ESIZE, ECUDA, ENOMEM, ENODEV = range(7)
-GEMM_AUTO, GEMM_SIMT, GEMM_TENSOR = 0, 1, 2
+GEMM_AUTO, GEMM_SIMT, GEMM_TENSOR, GEMM_TENSOR_SINGLE = 0, 1, 2, 3
 
 EXPORTED = [
     "negacyclic_last_error", "negacyclic_init", "negacyclic_get_info", "negacyclic_run",

@@ -21,6 +21,7 @@
 #include <cuda.h>
 
 #include <cstdio>
+#include <cstdlib>
 
 #include "gemm_tc.cuh"
 
@@ -156,6 +157,32 @@ __device__ __forceinline__ void tile_coords(uint32_t tile, const TileShape& shap
     const uint32_t rows_in_group = min(shape.group_m, shape.m_tiles - first_m);
     m_tile = first_m + within % rows_in_group;
     n_tile = within / rows_in_group;
+}
+
+// Applies the epilogue to 32 accumulator columns (c_base .. c_base+31) of one row.
+__device__ __forceinline__ void epilogue_chunk(const Epilogue& epi, const uint32_t (&v)[32], uint32_t c_base,
+                                               uint32_t columns, uint64_t out_row, uint32_t op, uint32_t column) {
+    if (epi.mode == kEpilogueRaw) {
+        int32_t* out = epi.raw + out_row * epi.raw_ld;
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (c_base + j < columns) out[c_base + j] = int32_t(v[j]);
+        return;
+    }
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+        const uint32_t group_index = c_base / 4 + g;
+        uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
+                     (uint64_t(v[4 * g + 3]) << 24);
+        if (epi.mode == kEpilogueConvert) {
+            if (group_index < epi.r) {
+                const DevicePrime f = epi.primes[group_index];
+                epi.residues[(size_t(op) * epi.r + group_index) * epi.n + column] = redc(s, f.p, f.pinv);
+            }
+        } else if (group_index < epi.words) {
+            epi.dots[out_row * epi.words + group_index] = s;
+        }
+    }
 }
 
 // Persistent, warp-specialised GEMM: each CTA walks tiles blockIdx.x, +gridDim.x, ...
@@ -314,27 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 uint32_t v[32];
                 tmem_load32(t_base + chunk * 32, v);
                 if (!row_ok) continue;
-                if (epi.mode == kEpilogueRaw) {
-                    int32_t* out = epi.raw + out_row * epi.raw_ld;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (c_base + j < shape.columns) out[c_base + j] = int32_t(v[j]);
-                    continue;
-                }
-#pragma unroll
-                for (int g = 0; g < 8; ++g) {
-                    const uint32_t group_index = c_base / 4 + g;
-                    uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) +
-                                 (uint64_t(v[4 * g + 2]) << 16) + (uint64_t(v[4 * g + 3]) << 24);
-                    if (epi.mode == kEpilogueConvert) {
-                        if (group_index < epi.r) {
-                            const DevicePrime f = epi.primes[group_index];
-                            epi.residues[(size_t(op) * epi.r + group_index) * epi.n + column] = redc(s, f.p, f.pinv);
-                        }
-                    } else if (group_index < epi.words) {
-                        epi.dots[out_row * epi.words + group_index] = s;
-                    }
-                }
+                epilogue_chunk(epi, v, c_base, shape.columns, out_row, op, column);
             }
             // every tcgen05.ld of this warp has completed (tmem_load32 waits): release the accumulator
             fence_before();
@@ -348,6 +355,257 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
     if (warp == 1) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kAccColumns)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pair (2-CTA) variant: a cluster of two CTAs computes a 256 x 256 tile with
+// tcgen05.mma.cta_group::2 (M = 256, N = 256). CTA rank r holds A rows
+// [128r, 128r+128) and B columns [128r, 128r+128) of the tile in its own shared
+// memory and rows [128r, 128r+128) of the accumulator in its own TMEM. Per MMA
+// each SM reads half the B bytes of the single-CTA kernel, and each stage
+// moves 32 KB per SM from L2 instead of 48 KB.
+//   * both CTAs' TMA loads complete on the leader's (rank 0) full[s] barrier,
+//     which the leader arms with both CTAs' bytes;
+//   * the leader's single MMA thread commits to empty[s] / acc_full[a] in both
+//     CTAs at once (tcgen05.commit ... multicast::cluster, mask 0b11);
+//   * all eight epilogue warps of the pair release an accumulator on the
+//     leader's acc_empty[a] (cluster-scope arrive).
+constexpr uint32_t kPairStages = 6;
+constexpr uint32_t kPairBlockN = 256;                      // columns per pair tile
+constexpr uint32_t kPairBTileBytes = (kPairBlockN / 2) * kBlockK;  // 16 KB: this CTA's half of B
+constexpr uint32_t kPairStageBytes = kATileBytes + kPairBTileBytes; // 32 KB per CTA
+constexpr size_t kPairSmemBytes = size_t(kPairStages) * kPairStageBytes + 1024 + 256;
+constexpr uint32_t kPairInstrDesc = (2u << 4) | ((kPairBlockN >> 3) << 17) | ((256u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    return rank;
+}
+
+__device__ __forceinline__ uint32_t leader_address(const void* local) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(0));
+    return remote;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int c0,
+                                                 int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+        "%5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int c0,
+                                                 int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t desc_a, uint64_t desc_b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(desc_a), "l"(desc_b), "r"(kPairInstrDesc), "r"(accumulate)
+        : "memory");
+}
+
+// arrive on the barrier at this shared-memory offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(uint16_t(3))
+        : "memory");
+}
+
+// arrive on this CTA's barrier once the pair MMAs issued so far have completed
+__device__ __forceinline__ void mma_commit_pair_local(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap a_map, const __grid_constant__ CUtensorMap b_map,
+                        TileShape shape, Epilogue epi) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* a_smem = smem;
+    uint8_t* b_smem = smem + kPairStages * kATileBytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(b_smem + kPairStages * kPairBTileBytes);
+    uint64_t* empty = full + kPairStages;
+    uint64_t* acc_full = empty + kPairStages;  // [2]
+    uint64_t* acc_empty = acc_full + 2;        // [2] (leader's are used)
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile uint32_t* abort_flag = tmem_slot + 1;
+
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const uint32_t pair = blockIdx.x / 2, pairs = gridDim.x / 2;
+    const uint32_t tiles = shape.m_tiles * shape.n_tiles;  // m_tiles counts 256-row pair tiles
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < kPairStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (uint32_t a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 2 * kEpilogueWarps);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * kAccColumns)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    cluster_sync();  // barriers and TMEM of both CTAs ready before any cross-CTA traffic
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer (both CTAs): own A half and B half, leader's barrier
+            uint32_t step = 0;
+            bool ok = true;
+            for (uint32_t tile = pair; tile < tiles && ok; tile += pairs) {
+                uint32_t m_tile, n_tile;
+                tile_coords(tile, shape, m_tile, n_tile);
+                const uint32_t row0 = m_tile * 256 + rank * kBlockM;
+                const uint32_t col0 = n_tile * kPairBlockN + rank * (kPairBlockN / 2);
+                uint32_t a_t = 0, a_row = shape.rows.first + row0;
+                if (shape.rows.mode == kRowsSplit) {
+                    uint32_t op, j;
+                    shape.rows.decompose(row0, op, a_t, j);
+                    a_row = op * shape.rows.n_sub + j;
+                }
+                for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
+                    const uint32_t s = step % kPairStages, round = step / kPairStages;
+                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                        ok = false;
+                        break;
+                    }
+                    if (leader) mbar_expect_tx(&full[s], 2 * kPairStageBytes);
+                    const uint32_t bar = leader_address(&full[s]);
+                    tma_load_3d_pair(a_smem + s * kATileBytes, &a_map, bar, int(ks * kBlockK), int(a_t), int(a_row));
+                    tma_load_2d_pair(b_smem + s * kPairBTileBytes, &b_map, bar, int(ks * kBlockK), int(col0));
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicOr(&g_tc_error, 16u);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---------------- MMA issuer (leader only)
+            uint32_t step = 0, local = 0;
+            bool ok = true;
+            for (uint32_t tile = pair; tile < tiles && ok; tile += pairs, ++local) {
+                const uint32_t acc = local & 1, use = local >> 1;
+                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t d_tmem = tmem + acc * kAccColumns;
+                for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
+                    const uint32_t s = step % kPairStages, round = step / kPairStages;
+                    if (*abort_flag || !mbar_wait(&full[s], round & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t a_addr = smem_u32(a_smem + s * kATileBytes);
+                    const uint32_t b_addr = smem_u32(b_smem + s * kPairBTileBytes);
+#pragma unroll
+                    for (uint32_t kk = 0; kk < kBlockK / 32; ++kk)
+                        mma_i8_pair(d_tmem, smem_descriptor(a_addr + kk * 32), smem_descriptor(b_addr + kk * 32),
+                                    (ks | kk) != 0 ? 1u : 0u);
+                    mma_commit_pair(&empty[s]);  // frees stage s in both CTAs
+                }
+                if (ok) mma_commit_pair(&acc_full[acc]);
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicOr(&g_tc_error, 32u);
+            }
+            mma_commit_pair_local(drain);  // every tcgen05 op here is cta_group::2
+            if (!mbar_wait(drain, 0)) atomicOr(&g_tc_error, 64u);
+        }
+    } else {
+        // ---------------- epilogue: this CTA's 128 rows of each pair tile
+        const uint32_t quarter = warp & 3;
+        const uint32_t release = leader_address(&acc_empty[0]);
+        uint32_t local = 0;
+        for (uint32_t tile = pair; tile < tiles; tile += pairs, ++local) {
+            const uint32_t acc = local & 1, use = local >> 1;
+            uint32_t m_tile, n_tile;
+            tile_coords(tile, shape, m_tile, n_tile);
+            const uint32_t row0 = m_tile * 256 + rank * kBlockM, col0 = n_tile * kPairBlockN;
+            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1);
+            have = __all_sync(0xffffffffu, have);
+            if (!have) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicOr(&g_tc_error, 128u);
+                }
+                break;
+            }
+            fence_after();
+            const uint32_t row = row0 + quarter * 32 + lane;
+            const bool row_ok = row < shape.m;
+            uint32_t op = 0, column = 0;
+            uint64_t out_row = 0;
+            if (row_ok) {
+                if (epi.mode == kEpilogueConvert)
+                    shape.rows.residue(row, op, column);
+                else
+                    out_row = shape.rows.row(row);
+            }
+            const uint32_t t_base = tmem + acc * kAccColumns + ((quarter * 32) << 16);
+            for (uint32_t chunk = 0; chunk < kPairBlockN / 32; ++chunk) {
+                const uint32_t c_base = col0 + chunk * 32;
+                if (c_base >= shape.columns) break;  // warp-uniform
+                uint32_t v[32];
+                tmem_load32(t_base + chunk * 32, v);
+                if (!row_ok) continue;
+                epilogue_chunk(epi, v, c_base, shape.columns, out_row, op, column);
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(release + acc * sizeof(uint64_t));
+        }
+    }
+    __syncwarp();
+    fence_before();
+    cluster_sync();  // the leader's MMAs have drained and no peer accesses remain
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kAccColumns)
                      : "memory");
     }
 }
@@ -426,19 +684,21 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     CUresult rb = encode(&plan.b_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(b), b_dims, b_strides,
                          b_box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (ra != CUDA_SUCCESS || rb != CUDA_SUCCESS) {
+    const cuuint32_t b_half_box[2] = {kBlockK, kPairBlockN / 2};
+    CUresult rh = encode(&plan.b_map_half, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(b), b_dims,
+                         b_strides, b_half_box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (ra != CUDA_SUCCESS || rb != CUDA_SUCCESS || rh != CUDA_SUCCESS) {
         why = "tensor map encoding failed";
         return false;
     }
-    static bool attribute_set = false;
-    if (!attribute_set) {
-        if (cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            why = "cannot reserve shared memory";
-            return false;
-        }
-        attribute_set = true;
+    if (cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(gemm_tc_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kPairSmemBytes)) != cudaSuccess) {
+        cudaGetLastError();
+        why = "cannot reserve shared memory";
+        return false;
     }
     plan.m = m;
     plan.columns = columns;
@@ -453,6 +713,10 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     plan.sm_count = sms > 0 ? uint32_t(sms) : 148;
+    // CTA pairs need 256-row slabs; NEGACYCLIC_GEMM_PAIRS=0 selects the single-CTA kernel
+    const char* pairs_env = getenv("NEGACYCLIC_GEMM_PAIRS");
+    plan.pairs = !(pairs_env && pairs_env[0] == '0') && plan.sm_count >= 2 &&
+                 (rows.mode == kRowsLinear || slab % 256 == 0);
     plan.ready = true;
     return true;
 }
@@ -466,15 +730,28 @@ bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_
 }
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
-                        uint32_t m) {
-    const uint32_t m_tiles = (m + kBlockM - 1) / kBlockM;
+                        uint32_t m, bool allow_pairs) {
+    const bool pairs = allow_pairs && plan.pairs && (rows.mode == kRowsLinear || rows.span % 256 == 0);
+    const uint32_t rows_per_tile = pairs ? 256 : kBlockM;
+    const uint32_t m_tiles = (m + rows_per_tile - 1) / rows_per_tile;
     // largest raster group whose A tiles fit comfortably in L2 (~48 MB)
-    uint64_t group = (48ull << 20) / plan.a_tile_bytes;
-    group = group < 8 ? 8 : (group > 64 ? 64 : group);
+    uint64_t group = (48ull << 20) / (plan.a_tile_bytes * (pairs ? 2 : 1));
+    group = group < 4 ? 4 : (group > 64 ? 64 : group);
     TileShape shape{m, plan.columns, plan.k_tiles, m_tiles, plan.n_tiles, uint32_t(group), rows};
     const uint32_t tiles = m_tiles * plan.n_tiles;
+    if (pairs) {
+        const uint32_t max_pairs = plan.sm_count / 2;
+        const uint32_t grid = 2 * (tiles < max_pairs ? tiles : max_pairs);
+        gemm_tc_pair_kernel<<<grid, kThreads, kPairSmemBytes, stream>>>(plan.a_map, plan.b_map_half, shape, epilogue);
+        return;
+    }
     const uint32_t grid = tiles < plan.sm_count ? tiles : plan.sm_count;
     gemm_tc_kernel<<<grid, kThreads, kSmemBytes, stream>>>(plan.a_map, plan.b_map, shape, epilogue);
+}
+
+void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
+                        uint32_t m) {
+    launch_gemm_tensor(plan, epilogue, stream, rows, m, true);
 }
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {

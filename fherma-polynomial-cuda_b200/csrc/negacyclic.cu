@@ -469,12 +469,12 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
     raw.raw_ld = n;
     RowMap rows = RowMap::linear(0);
     try {
-        if (engine == NEGACYCLIC_GEMM_TENSOR) {
+        if (engine == NEGACYCLIC_GEMM_TENSOR || engine == NEGACYCLIC_GEMM_TENSOR_SINGLE) {
             TensorGemmPlan plan;
             std::string why;
             if (!prepare_gemm_tensor(plan, d_a, k, rows, m, d_b, n, k, why))
                 return fail(NEGACYCLIC_EINVAL, "tensor GEMM unavailable: " + why);
-            launch_gemm_tensor(plan, raw, stream);
+            launch_gemm_tensor(plan, raw, stream, rows, m, engine == NEGACYCLIC_GEMM_TENSOR);
         } else {
             launch_gemm_simt(d_a, k, rows, m, d_b, n, k, raw, stream);
         }

@@ -44,7 +44,8 @@ extern "C" {
 /* GEMM engine for the two byte-sliced products (conversion and CRT). */
 #define NEGACYCLIC_GEMM_AUTO 0   /* tensor cores where the shape allows it */
 #define NEGACYCLIC_GEMM_SIMT 1   /* dp4a CUDA-core kernel (any shape) */
-#define NEGACYCLIC_GEMM_TENSOR 2 /* tcgen05 kind::i8, TMA-fed, TMEM accumulators */
+#define NEGACYCLIC_GEMM_TENSOR 2 /* tcgen05 kind::i8, TMA-fed, TMEM accumulators (CTA pairs where possible) */
+#define NEGACYCLIC_GEMM_TENSOR_SINGLE 3 /* negacyclic_gemm_u8 only: the single-CTA tcgen05 kernel */
 
 typedef struct negacyclic_plan negacyclic_plan;
 

@@ -26,7 +26,8 @@ def torch():
 
 # ---------------------------------------------------------------- raw byte GEMM
 
-@pytest.mark.parametrize("m,n,k", [(128, 256, 128), (300, 520, 400), (1024, 768, 2048), (256, 512, 33024)])
+@pytest.mark.parametrize("m,n,k", [(128, 256, 128), (300, 520, 400), (1024, 768, 2048), (256, 512, 33024),
+                                   (4096, 1280, 1024)])
 def test_tensor_gemm_matches_simt_and_numpy(m, n, k, fpc, torch):
     gen = torch.Generator(device="cuda").manual_seed(m + n + k)
     a = torch.randint(0, 256, (m, k), dtype=torch.uint8, device="cuda", generator=gen)
@@ -36,7 +37,7 @@ def test_tensor_gemm_matches_simt_and_numpy(m, n, k, fpc, torch):
         b[0].fill_(255)
     outs = {}
     lib = fpc.library()
-    for engine in (fpc.GEMM_SIMT, fpc.GEMM_TENSOR):
+    for engine in (fpc.GEMM_SIMT, fpc.GEMM_TENSOR, fpc.GEMM_TENSOR_SINGLE):
         d = torch.full((m, n), -1, dtype=torch.int32, device="cuda")
         status = lib.negacyclic_gemm_u8(a.data_ptr(), b.data_ptr(), d.data_ptr(), m, n, k, engine, None)
         assert status == 0, fpc.last_error()
@@ -44,7 +45,8 @@ def test_tensor_gemm_matches_simt_and_numpy(m, n, k, fpc, torch):
         outs[engine] = d.cpu().numpy()
     want = a.cpu().numpy().astype(np.int64) @ b.cpu().numpy().astype(np.int64).T
     assert np.array_equal(outs[fpc.GEMM_SIMT].astype(np.int64), want)
-    assert np.array_equal(outs[fpc.GEMM_TENSOR].astype(np.int64), want)
+    assert np.array_equal(outs[fpc.GEMM_TENSOR].astype(np.int64), want)  # CTA-pair kernel
+    assert np.array_equal(outs[fpc.GEMM_TENSOR_SINGLE].astype(np.int64), want)
 
 
 # ---------------------------------------------------------------- reference checker points
