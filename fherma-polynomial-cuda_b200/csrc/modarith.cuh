@@ -19,20 +19,23 @@ struct DevicePrime {
     uint32_t r2;        // 2^64 mod p
 };
 
-__device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b, uint32_t p) {
-    uint32_t t = a + b;
-    return t >= p ? t - p : t;
-}
+// Conditional subtractions as unsigned minima: for t in [0, 2p) with 2p < 2^32,
+// t - p wraps above t exactly when t < p, so min(t, t - p) is t mod p.
+__device__ __forceinline__ uint32_t reduce_once(uint32_t t, uint32_t p) { return min(t, t - p); }
 
+__device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b, uint32_t p) { return reduce_once(a + b, p); }
+
+// a, b in [0, p): a - b wraps when a < b, and then a - b + p is the smaller value
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t p) {
-    return a >= b ? a - b : a + p - b;
+    const uint32_t t = a - b;
+    return min(t, t + p);
 }
 
 // t < p * 2^32  ->  t * 2^-32 mod p, canonical
 __device__ __forceinline__ uint32_t redc(uint64_t t, uint32_t p, uint32_t pinv) {
     uint32_t m = uint32_t(t) * pinv;
     uint32_t u = uint32_t((t + uint64_t(m) * p) >> 32);
-    return u >= p ? u - p : u;
+    return reduce_once(u, p);
 }
 
 __device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
@@ -43,7 +46,7 @@ __device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uin
 __device__ __forceinline__ uint32_t shoup(uint32_t a, uint32_t w, uint32_t w_q, uint32_t p) {
     uint32_t quotient = __umulhi(a, w_q);
     uint32_t r = a * w - quotient * p;
-    return r >= p ? r - p : r;
+    return reduce_once(r, p);
 }
 
 // base^e mod p in standard form, via Montgomery squaring
