@@ -303,6 +303,155 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+SIZES = (4096, 8192, 16384, 32768, 65536)
+
+
+def uneven_instances(count: int, seed: int):
+    """Instances of the batched configuration: N uniform over SIZES, L log-uniform in [32, 1747],
+    a distinct random odd q per instance (top limb nonzero), a and b uniform in [0, q)."""
+    inputs = load_inputs()
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        n = int(rng.choice(SIZES))
+        limbs = int(np.floor(np.exp(rng.uniform(np.log(32), np.log(1748)))))
+        q, a, b = inputs.instance(n, min(limbs, 1747), seed * 1000 + i, 0)
+        out.append((n, q.shape[0], q, a, b))
+    return out
+
+
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def run_batch(args):
+    """64 uneven products: one graph launch (batched) against one call per product (plain)."""
+    import ctypes
+
+    import torch
+
+    torch.cuda.set_device(0)
+    fpc = _load("fpc_b200", os.path.join(PACKAGE_DIR, "__init__.py"), PACKAGE_DIR)
+    t0 = time.perf_counter()
+    instances = uneven_instances(args.count, 100)
+    log(f"generated {len(instances)} instances in {time.perf_counter() - t0:.1f} s")
+    cudart = ctypes.CDLL("libcudart.so.12")
+    cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    batch = fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in instances], lanes=args.lanes, tune=args.tune,
+                      tune_cache=args.tune_cache)
+    setup_s = time.perf_counter() - t0
+    log(f"batch created ({setup_s:.1f} s since start)")
+    for i, (n, l, q, a, b) in enumerate(instances):
+        da, db, _ = batch.io(i)
+        cudart.cudaMemcpy(da, a.ctypes.data, a.nbytes, 1)
+        cudart.cudaMemcpy(db, b.ctypes.data, b.nbytes, 1)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t1 = time.perf_counter()
+    batch.run_device(sptr)
+    torch.cuda.synchronize()
+    log(f"first batch run {time.perf_counter() - t1:.2f} s, pipeline status {fpc.pipeline_status()}")
+    for _ in range(args.warmup):
+        batch.run_device(sptr)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        batch.run_device(sptr)
+    stop.record(stream)
+    stop.synchronize()
+    batched_ms = start.elapsed_time(stop) / args.steps
+    log(f"batched {batched_ms:.1f} ms per batch, pipeline status {fpc.pipeline_status()}")
+    # plain per-call path: one product per call, each call completing before the next
+    plain_ms = 0.0
+    for _ in range(max(1, args.steps // 2)):
+        start.record(stream)
+        for i in range(len(instances)):
+            batch.run_one(i, sptr)
+            stream.synchronize()
+        stop.record(stream)
+        stop.synchronize()
+        plain_ms += start.elapsed_time(stop) / max(1, args.steps // 2)
+    log(f"plain {plain_ms:.1f} ms per batch, pipeline status {fpc.pipeline_status()}")
+    ops = sum(2.0 * (2 * n) * (4 * l) * (4 * batch.info(i)["primes"]) + 2.0 * n * (4 * batch.info(i)["primes"]) *
+              (4 * (l + 5)) for i, (n, l, *_r) in enumerate(instances))
+    line = {"metric": f"products/s, {len(instances)} uneven products (N in 4096..65536, L log-uniform 32..1747)",
+            "value": len(instances) / (batched_ms / 1000), "unit": "products/s", "mode": "batched graph",
+            "plain_value": len(instances) / (plain_ms / 1000), "batched_over_plain": plain_ms / batched_ms,
+            "ms_per_batch": batched_ms, "plain_ms_per_batch": plain_ms, "int8_tops": ops / (batched_ms / 1000) / 1e12,
+            "lanes": args.lanes or min(len(instances), 4), "tuned": bool(args.tune), "setup_s": setup_s,
+            "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seed 100)"}
+    print(json.dumps(line), flush=True)
+    batch.close()
+
+
+def run_serve(args):
+    """Poisson arrivals over 8 sessions (fixed L and q each, N per request); p50/p99 and products/s."""
+    import torch
+
+    torch.cuda.set_device(0)
+    fpc = _load("fpc_b200", os.path.join(PACKAGE_DIR, "__init__.py"), PACKAGE_DIR)
+    inputs = load_inputs()
+    rng = np.random.Generator(np.random.PCG64(200))
+    max_limbs = args.serve_max_limbs
+    sessions = []
+    server = fpc.Server(hbm_budget=int(args.budget_gb * (1 << 30)), slots=args.slots)
+    for sidx in range(8):
+        limbs = int(np.floor(np.exp(rng.uniform(np.log(32), np.log(max_limbs + 1)))))
+        q = inputs.random_modulus(limbs, 200 + sidx)
+        sid = server.open_session(32 * limbs, limbs, q, ns=SIZES)
+        pool = {}
+        log(f"session {sidx}: L={limbs}")
+        for n in SIZES:  # page-locked operand pairs per ring size
+            pairs = []
+            for k in range(args.serve_pairs):
+                a = torch.from_numpy(inputs.random_operand(rng, n, q).view(np.int32)).pin_memory()
+                b = torch.from_numpy(inputs.random_operand(rng, n, q).view(np.int32)).pin_memory()
+                pairs.append((a.numpy().view(np.uint32), b.numpy().view(np.uint32)))
+            pool[n] = pairs
+        sessions.append((sid, limbs, pool))
+    outputs = {}
+    for sid, limbs, pool in sessions:
+        for n in SIZES:
+            outputs[(sid, n)] = [torch.empty((n, limbs), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+                                 for _ in range(args.slots + 1)]
+    log("sessions and buffers ready")
+    # Poisson arrival schedule
+    t = 0.0
+    schedule = []
+    while t < args.duration:
+        t += rng.exponential(1.0 / args.rate)
+        s_index = int(rng.integers(len(sessions)))
+        schedule.append((t, s_index, int(rng.choice(SIZES)), int(rng.integers(args.serve_pairs))))
+    ids = []
+    out_counter = {}
+    start = time.perf_counter()
+    for when, s_index, n, k in schedule:
+        delay = when - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        sid, limbs, pool = sessions[s_index]
+        ring = outputs[(sid, n)]
+        slot = out_counter.get((sid, n), 0)
+        out_counter[(sid, n)] = slot + 1
+        a, b = pool[n][k]
+        ids.append(server.submit(sid, a, b, out=ring[slot % len(ring)]))
+    log(f"submitted {len(ids)} requests")
+    latencies = [server.wait(rid)[1] for rid in ids]
+    elapsed = time.perf_counter() - start
+    log(f"all done in {elapsed:.1f} s, pipeline status {fpc.pipeline_status()}")
+    stats = server.stats()
+    server.close()
+    lat = np.array(latencies)
+    line = {"metric": f"served products/s at {args.rate:g} req/s Poisson, 8 sessions, N in 4096..65536",
+            "value": len(ids) / elapsed, "unit": "products/s", "mode": "serving (continuous batching)",
+            "requests": len(ids), "offered_rate": args.rate, "duration_s": elapsed,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "slots": args.slots, "hbm_budget_gb": args.budget_gb,
+            "session_max_limbs": max_limbs, "failed": stats["failed"], "data": "synthetic (seed 200)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -314,10 +463,26 @@ def main():
                         help="N,L of a smaller case for profiling (the benchmark line is N=65536,L=1747)")
     parser.add_argument("--device-only", action="store_true",
                         help="device-resident products and stage times only (profiling runs)")
+    parser.add_argument("--mode", choices=("plain", "batch", "serve"), default="plain",
+                        help="plain: the benchmark line; batch / serve: the batched and serving forms")
+    parser.add_argument("--count", type=int, default=64, help="batch: number of uneven products")
+    parser.add_argument("--lanes", type=int, default=0, help="batch: concurrent streams (0 = 4)")
+    parser.add_argument("--tune", action="store_true", help="batch: run the autotuner for uncached shapes")
+    parser.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
+    parser.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
+    parser.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    parser.add_argument("--slots", type=int, default=4, help="serve: concurrent requests")
+    parser.add_argument("--budget-gb", type=float, default=60.0, help="serve: HBM budget (GiB)")
+    parser.add_argument("--serve-max-limbs", type=int, default=1747, help="serve: largest session L")
+    parser.add_argument("--serve-pairs", type=int, default=1, help="serve: operand pairs per (session, N)")
     args = parser.parse_args()
     args.n, args.limbs = (int(x) for x in args.workload.split(","))
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "batch":
+        run_batch(args)
+    elif args.mode == "serve":
+        run_serve(args)
     else:
         run_b200(args)
 

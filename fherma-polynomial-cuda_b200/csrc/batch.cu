@@ -1,0 +1,384 @@
+// Batched form: many products of uneven (N, L, q) in one graph-captured launch.
+//
+// The reference runs one product per harness call (src/main.cpp:164-204) and has
+// no batched form; this is new work on top of the same per-product pipeline.
+//
+//   * one plan per instance (parameter tables resident), work space external;
+//   * an autotuner picks, per shape (N, L), the ring split s (which sets the NTT
+//     length N' = N/s and the prime set) and the GEMM kernel (CTA-pair 256x256
+//     tiles, single-CTA 128x256 tiles, or the SIMT kernel) by timing each
+//     candidate on the device; results are cached in a text file;
+//   * instances are assigned longest-first to `lanes` streams; each lane owns
+//     one work arena (sized for its largest instance) that its instances use
+//     one after another;
+//   * the whole batch — every lane's chain of products — is captured once into a
+//     CUDA graph, so a batch run is a single cudaGraphLaunch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "plan_internal.h"
+
+using namespace negacyclic;
+using namespace negacyclic::detail;
+
+namespace {
+
+struct TuneChoice {
+    uint32_t split = 0;  // 0 = automatic
+    uint32_t gemm = NEGACYCLIC_GEMM_AUTO;
+    double ms = 0;  // measured device time of one product (0 = not measured)
+};
+
+using ShapeKey = std::pair<uint32_t, uint32_t>;  // (N, L)
+
+std::mutex g_cache_mutex;
+
+std::map<ShapeKey, TuneChoice> load_cache(const std::string& path) {
+    std::map<ShapeKey, TuneChoice> cache;
+    if (path.empty()) return cache;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream fields(line);
+        uint32_t n = 0, limbs = 0;
+        TuneChoice c;
+        if (fields >> n >> limbs >> c.split >> c.gemm >> c.ms) cache[{n, limbs}] = c;
+    }
+    return cache;
+}
+
+void save_cache(const std::string& path, const std::map<ShapeKey, TuneChoice>& cache) {
+    if (path.empty()) return;
+    std::ofstream out(path, std::ios::trunc);
+    out.precision(17);
+    out << "# N L split gemm ms  (negacyclic batch autotuner)\n";
+    for (const auto& [key, c] : cache)
+        out << key.first << ' ' << key.second << ' ' << c.split << ' ' << c.gemm << ' ' << c.ms << '\n';
+}
+
+// Device time of one product for a plan (operands uninitialised: the arithmetic
+// is data-independent apart from the rare final corrections).
+double time_plan(negacyclic_plan& plan, int repeats) {
+    const HostPlan& h = plan.host;
+    const size_t words = size_t(h.n) * h.limbs;
+    uint32_t* io = nullptr;
+    check(cudaMalloc(&io, 3 * words * sizeof(uint32_t)), "cudaMalloc");
+    check(cudaMemset(io, 0x5a, 3 * words * sizeof(uint32_t)), "cudaMemset");
+    cudaEvent_t start = nullptr, stop = nullptr;
+    check(cudaEventCreate(&start), "cudaEventCreate");
+    check(cudaEventCreate(&stop), "cudaEventCreate");
+    cudaStream_t st = plan.stream;
+    enqueue_device_product(plan, io, io + words, io + 2 * words, st);  // warm-up
+    check(cudaEventRecord(start, st), "cudaEventRecord");
+    for (int i = 0; i < repeats; ++i) enqueue_device_product(plan, io, io + words, io + 2 * words, st);
+    check(cudaEventRecord(stop, st), "cudaEventRecord");
+    check(cudaEventSynchronize(stop), "tuning products");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, start, stop), "cudaEventElapsedTime");
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    cudaFree(io);
+    return double(ms) / repeats;
+}
+
+// Candidate (split, gemm) pairs for a shape, timed with the instance's own q.
+TuneChoice tune_shape(const negacyclic_point& point, int device) {
+    std::vector<uint32_t> splits;
+    {
+        HostPlan probe;
+        std::string error;
+        int status = 0;
+        if (!build_host_plan(point.n, point.limbs, point.q, 0, probe, error, status)) return TuneChoice{};
+        splits.push_back(probe.split);
+        const uint32_t wider = probe.split * 2;
+        if (wider <= kMaxSplit && point.n / wider >= 256) splits.push_back(wider);
+    }
+    TuneChoice best;
+    for (uint32_t split : splits) {
+        for (uint32_t gemm : {uint32_t(NEGACYCLIC_GEMM_AUTO), uint32_t(NEGACYCLIC_GEMM_TENSOR_SINGLE),
+                              uint32_t(NEGACYCLIC_GEMM_SIMT)}) {
+            // the SIMT GEMM only competes on small shapes: skip it where tensor cores apply
+            if (gemm == NEGACYCLIC_GEMM_SIMT && best.ms > 0 && uint64_t(point.n) * point.limbs > (1u << 16)) continue;
+            negacyclic_options o{};
+            o.split = split;
+            o.gemm = gemm;
+            o.device = device;
+            negacyclic_plan* plan = nullptr;
+            if (negacyclic_init(point.n, point.w, point.limbs, point.q, &o, &plan) != NEGACYCLIC_OK) continue;
+            std::unique_ptr<negacyclic_plan> owner(plan);
+            double ms = 0;
+            try {
+                ms = time_plan(*plan, 3);
+            } catch (const CudaError&) {
+                cudaGetLastError();
+                continue;
+            }
+            if (best.ms == 0 || ms < best.ms) best = TuneChoice{split, gemm, ms};
+        }
+    }
+    return best;
+}
+
+// Rough device time of one product, for balancing lanes when nothing was measured.
+double estimate_ms(const negacyclic_plan& plan) {
+    const HostPlan& h = plan.host;
+    const double ops = 2.0 * (2.0 * h.n) * (4.0 * h.limbs) * (4.0 * plan.r) + 2.0 * h.n * (4.0 * plan.r) * (4.0 * h.words);
+    const double bytes = 16.0 * plan.r * double(h.n) * 4;
+    return ops / 2.0e15 * 1e3 + bytes / 4.0e12 * 1e3 + 0.05;
+}
+
+}  // namespace
+
+struct negacyclic_batch {
+    int device = 0;
+    std::vector<std::unique_ptr<negacyclic_plan>> plans;
+    std::vector<TuneChoice> choices;
+    std::vector<uint32_t> lane_of;
+    std::vector<std::vector<uint32_t>> lane_order;
+    std::vector<cudaStream_t> lanes;
+    std::vector<void*> arenas;
+    void* io = nullptr;
+    std::vector<size_t> io_offset;  // a, then b, then c per instance
+    cudaStream_t capture = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    ~negacyclic_batch() {
+        int previous = 0;
+        cudaGetDevice(&previous);
+        cudaSetDevice(device);
+        cudaDeviceSynchronize();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (cudaStream_t s : lanes) cudaStreamDestroy(s);
+        if (capture) cudaStreamDestroy(capture);
+        for (void* a : arenas) cudaFree(a);
+        if (io) cudaFree(io);
+        plans.clear();
+        cudaSetDevice(previous);
+    }
+
+    size_t words(uint32_t i) const { return size_t(plans[i]->host.n) * plans[i]->host.limbs; }
+    uint32_t* slot(uint32_t i, uint32_t which) const {
+        return reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(io) + io_offset[3 * i + which]);
+    }
+};
+
+extern "C" {
+
+int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, const negacyclic_batch_options* opts,
+                            negacyclic_batch** out) {
+    if (!points || !count || !out) return fail(NEGACYCLIC_EINVAL, "NULL or empty batch");
+    *out = nullptr;
+    negacyclic_batch_options o{};
+    o.device = -1;
+    if (opts) o = *opts;
+    int device = o.device;
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(NEGACYCLIC_ENODEV, "no CUDA device");
+    auto b = std::make_unique<negacyclic_batch>();
+    b->device = device;
+    DeviceGuard guard(device);
+    const std::string cache_path = o.tune_cache ? o.tune_cache : (getenv("NEGACYCLIC_TUNE_CACHE") ? getenv("NEGACYCLIC_TUNE_CACHE") : "");
+    try {
+        // 1. choices per shape (tuned or cached), then one plan per instance
+        std::map<ShapeKey, TuneChoice> cache;
+        {
+            std::lock_guard<std::mutex> lock(g_cache_mutex);
+            cache = load_cache(cache_path);
+        }
+        bool cache_dirty = false;
+        b->choices.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            const ShapeKey key{points[i].n, points[i].limbs};
+            auto it = cache.find(key);
+            if (it == cache.end() && o.tune) {
+                TuneChoice c = tune_shape(points[i], device);
+                it = cache.emplace(key, c).first;
+                cache_dirty = true;
+            }
+            b->choices[i] = it == cache.end() ? TuneChoice{} : it->second;
+            negacyclic_options po{};
+            po.split = b->choices[i].split;
+            po.gemm = b->choices[i].gemm;
+            po.device = device;
+            po.external_work = 1;
+            negacyclic_plan* plan = nullptr;
+            int status = negacyclic_init(points[i].n, points[i].w, points[i].limbs, points[i].q, &po, &plan);
+            if (status != NEGACYCLIC_OK && (po.split || po.gemm)) {  // a stale cache entry: fall back to defaults
+                po.split = 0;
+                po.gemm = NEGACYCLIC_GEMM_AUTO;
+                b->choices[i] = TuneChoice{};
+                status = negacyclic_init(points[i].n, points[i].w, points[i].limbs, points[i].q, &po, &plan);
+            }
+            if (status != NEGACYCLIC_OK)
+                return fail(status, "batch instance " + std::to_string(i) + ": " + negacyclic_last_error());
+            b->plans.emplace_back(plan);
+        }
+        if (cache_dirty) {
+            std::lock_guard<std::mutex> lock(g_cache_mutex);
+            save_cache(cache_path, cache);
+        }
+
+        // 2. longest-first assignment to lanes
+        const uint32_t lanes = o.lanes ? std::min(o.lanes, count) : std::min<uint32_t>(count, 4);
+        // Products on several lanes run concurrently: they use the single-CTA tensor-core kernel,
+        // because concurrent launches of the CTA-pair (cluster) kernel from several streams stalled.
+        if (lanes > 1)
+            for (auto& plan : b->plans) plan->gemm_pairs_allowed = false;
+        std::vector<double> cost(count);
+        for (uint32_t i = 0; i < count; ++i)
+            cost[i] = b->choices[i].ms > 0 ? b->choices[i].ms : estimate_ms(*b->plans[i]);
+        std::vector<uint32_t> order(count);
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
+        std::vector<double> load(lanes, 0.0);
+        b->lane_of.assign(count, 0);
+        b->lane_order.assign(lanes, {});
+        for (uint32_t i : order) {
+            const uint32_t lane = uint32_t(std::min_element(load.begin(), load.end()) - load.begin());
+            load[lane] += cost[i];
+            b->lane_of[i] = lane;
+            b->lane_order[lane].push_back(i);
+        }
+
+        // 3. device memory: one work arena per lane, one I/O arena for every instance
+        b->lanes.resize(lanes);
+        b->arenas.assign(lanes, nullptr);
+        for (uint32_t lane = 0; lane < lanes; ++lane) {
+            check(cudaStreamCreateWithFlags(&b->lanes[lane], cudaStreamNonBlocking), "cudaStreamCreate");
+            size_t need = 256;
+            for (uint32_t i : b->lane_order[lane]) need = std::max(need, b->plans[i]->work_bytes);
+            check(cudaMalloc(&b->arenas[lane], need), "cudaMalloc");
+            for (uint32_t i : b->lane_order[lane]) {
+                const std::string why = bind_work(*b->plans[i], b->arenas[lane]);
+                if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
+            }
+        }
+        size_t io_bytes = 0;
+        b->io_offset.resize(3 * size_t(count));
+        for (uint32_t i = 0; i < count; ++i)
+            for (uint32_t which = 0; which < 3; ++which) {
+                b->io_offset[3 * i + which] = io_bytes;
+                io_bytes += (b->words(i) * 4 + 255) / 256 * 256;
+            }
+        check(cudaMalloc(&b->io, io_bytes), "cudaMalloc");
+        check(cudaMemset(b->io, 0, io_bytes), "cudaMemset");
+
+        // 4. capture every lane's chain of products into one graph
+        check(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate");
+        b->joins.resize(lanes);
+        for (auto& e : b->joins) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        try {
+            check(cudaEventRecord(b->fork, b->capture), "cudaEventRecord");
+            for (uint32_t lane = 0; lane < lanes; ++lane) {
+                check(cudaStreamWaitEvent(b->lanes[lane], b->fork, 0), "cudaStreamWaitEvent");
+                for (uint32_t i : b->lane_order[lane])
+                    enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), b->lanes[lane]);
+                check(cudaEventRecord(b->joins[lane], b->lanes[lane]), "cudaEventRecord");
+                check(cudaStreamWaitEvent(b->capture, b->joins[lane], 0), "cudaStreamWaitEvent");
+            }
+        } catch (...) {
+            cudaGraph_t abandoned = nullptr;
+            cudaStreamEndCapture(b->capture, &abandoned);
+            if (abandoned) cudaGraphDestroy(abandoned);
+            throw;
+        }
+        check(cudaStreamEndCapture(b->capture, &b->graph), "cudaStreamEndCapture");
+        check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+        check(cudaGraphUpload(b->exec, b->capture), "cudaGraphUpload");
+        check(cudaStreamSynchronize(b->capture), "cudaGraphUpload");
+    } catch (const CudaError& e) {
+        cudaGetLastError();
+        return e.code == cudaErrorMemoryAllocation ? fail(NEGACYCLIC_ENOMEM, "device allocation failed")
+                                                   : cuda_failure(e);
+    }
+    *out = b.release();
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_io(negacyclic_batch* b, uint32_t index, uint32_t** d_a, uint32_t** d_b, uint32_t** d_c) {
+    if (!b || index >= b->plans.size()) return fail(NEGACYCLIC_EINVAL, "bad batch index");
+    if (d_a) *d_a = b->slot(index, 0);
+    if (d_b) *d_b = b->slot(index, 1);
+    if (d_c) *d_c = b->slot(index, 2);
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_get_info(const negacyclic_batch* b, uint32_t index, negacyclic_batch_instance* info) {
+    if (!b || !info || index >= b->plans.size()) return fail(NEGACYCLIC_EINVAL, "bad batch index");
+    *info = negacyclic_batch_instance{};
+    negacyclic_get_info(b->plans[index].get(), &info->plan);
+    info->lane = b->lane_of[index];
+    info->tuned_ms = b->choices[index].ms;
+    info->requested_gemm = b->choices[index].gemm;
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_run_device(negacyclic_batch* b, void* stream) {
+    if (!b) return fail(NEGACYCLIC_EINVAL, "NULL batch");
+    DeviceGuard guard(b->device);
+    const cudaError_t e = cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(NEGACYCLIC_ECUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_run_one(negacyclic_batch* b, uint32_t index, void* stream) {
+    if (!b || index >= b->plans.size()) return fail(NEGACYCLIC_EINVAL, "bad batch index");
+    DeviceGuard guard(b->device);
+    try {
+        enqueue_device_product(*b->plans[index], b->slot(index, 0), b->slot(index, 1), b->slot(index, 2),
+                               static_cast<cudaStream_t>(stream));
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const uint32_t* const* bb, uint32_t* const* c) {
+    if (!b || !a || !bb || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    DeviceGuard guard(b->device);
+    try {
+        // per lane: copy in, product, copy out, instance after instance; lanes overlap each other
+        const uint32_t count = uint32_t(b->plans.size());
+        size_t issued = 0;
+        std::vector<size_t> next(b->lanes.size(), 0);
+        while (issued < count) {  // round-robin issue so pageable copies of one lane overlap the others' compute
+            for (uint32_t lane = 0; lane < b->lanes.size(); ++lane) {
+                if (next[lane] >= b->lane_order[lane].size()) continue;
+                const uint32_t i = b->lane_order[lane][next[lane]++];
+                const size_t bytes = b->words(i) * 4;
+                cudaStream_t st = b->lanes[lane];
+                check(cudaMemcpyAsync(b->slot(i, 0), a[i], bytes, cudaMemcpyHostToDevice, st), "copy a");
+                check(cudaMemcpyAsync(b->slot(i, 1), bb[i], bytes, cudaMemcpyHostToDevice, st), "copy b");
+                enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), st);
+                check(cudaMemcpyAsync(c[i], b->slot(i, 2), bytes, cudaMemcpyDeviceToHost, st), "copy c");
+                ++issued;
+            }
+        }
+        for (cudaStream_t st : b->lanes) check(cudaStreamSynchronize(st), "batch");
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
+    return NEGACYCLIC_OK;
+}
+
+void negacyclic_batch_free(negacyclic_batch* b) { delete b; }
+
+}  // extern "C"

@@ -20,10 +20,11 @@
 #include "gemm_tc.cuh"
 #include "host_plan.h"
 #include "kernels.cuh"
+#include "plan_internal.h"
 
 using namespace negacyclic;
 
-namespace {
+namespace negacyclic::detail {
 
 thread_local std::string g_error;
 
@@ -31,11 +32,6 @@ int fail(int status, const std::string& message) {
     g_error = message;
     return status;
 }
-
-struct CudaError {
-    cudaError_t code;
-    const char* where;
-};
 
 void check(cudaError_t code, const char* where) {
     if (code != cudaSuccess) throw CudaError{code, where};
@@ -50,50 +46,11 @@ void device_alloc(T*& ptr, size_t count, size_t& counter) {
 
 uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 
-}  // namespace
+}  // namespace negacyclic::detail
 
-struct negacyclic_plan {
-    int device = 0;
-    HostPlan host;
-    uint32_t r = 0, padded_r = 0, padded_limbs = 0, k_convert = 0, k_crt = 0, crt_columns = 0;
-    uint32_t convert_engine = NEGACYCLIC_GEMM_SIMT, crt_engine = NEGACYCLIC_GEMM_SIMT;
-    DevicePrime* primes = nullptr;
-    uint2 *fwd = nullptr, *inv = nullptr, *zeta = nullptr;
-    uint8_t *convert_weights = nullptr, *crt_weights = nullptr;
-    uint32_t *q = nullptr, *minus_p = nullptr, *crt_words = nullptr;
-    uint32_t *operands = nullptr, *residues = nullptr, *crt_in = nullptr, *result = nullptr;
-    uint64_t* dots = nullptr;
-    uint32_t* error_flag = nullptr;
-    cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
-    static constexpr uint32_t kMaxChunks = 16;
-    uint32_t chunks = 1;  // coefficient chunks of the streamed host path
-    cudaEvent_t in_ready[kMaxChunks] = {}, out_ready[kMaxChunks] = {};
-    size_t device_bytes = 0, table_bytes = 0;
-    TensorGemmPlan convert_gemm, crt_gemm;
+using namespace negacyclic::detail;
 
-    ~negacyclic_plan() {
-        int previous = 0;
-        cudaGetDevice(&previous);
-        cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
-        void* buffers[] = {primes, fwd, inv, zeta, convert_weights, crt_weights, q, minus_p, crt_words,
-                           operands, residues, crt_in, result, dots, error_flag};
-        for (void* ptr : buffers)
-            if (ptr) cudaFree(ptr);
-        if (copy_in) cudaStreamSynchronize(copy_in);
-        if (copy_out) cudaStreamSynchronize(copy_out);
-        for (uint32_t c = 0; c < kMaxChunks; ++c) {
-            if (in_ready[c]) cudaEventDestroy(in_ready[c]);
-            if (out_ready[c]) cudaEventDestroy(out_ready[c]);
-        }
-        if (stream) cudaStreamDestroy(stream);
-        if (copy_in) cudaStreamDestroy(copy_in);
-        if (copy_out) cudaStreamDestroy(copy_out);
-        cudaSetDevice(previous);
-    }
-};
-
-namespace {
+namespace negacyclic::detail {
 
 constexpr uint32_t kStages = 7;  // convert, forward, pointwise, inverse, transpose, crt, reduce
 
@@ -175,22 +132,74 @@ void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cud
     check(cudaGetLastError(), "product kernels");
 }
 
+// Work-space layout of one product (256-byte aligned pieces).
+struct WorkLayout {
+    size_t operands, residues, crt_in, dots, result, error_flag, total;
+};
+
+WorkLayout work_layout(const negacyclic_plan& s) {
+    const HostPlan& h = s.host;
+    auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+    WorkLayout w{};
+    size_t at = 0;
+    w.operands = at;
+    at = align(at + size_t(2) * h.n * s.padded_limbs * 4);
+    w.residues = at;
+    at = align(at + size_t(2) * s.r * h.n * 4);
+    w.crt_in = at;
+    at = align(at + size_t(h.n) * s.padded_r * 4);
+    w.dots = at;
+    at = align(at + size_t(h.n) * h.words * 8);
+    w.result = at;
+    at = align(at + size_t(h.n) * h.limbs * 4);
+    w.error_flag = at;
+    at = align(at + 4);
+    w.total = at;
+    return w;
+}
+
+// Points the plan at a work space and re-encodes the GEMM tensor maps for it.
+// Returns an error message, or "" on success.
+std::string bind_work(negacyclic_plan& s, void* arena) {
+    const HostPlan& h = s.host;
+    const WorkLayout w = work_layout(s);
+    uint8_t* base = static_cast<uint8_t*>(arena);
+    s.operands = reinterpret_cast<uint32_t*>(base + w.operands);
+    s.residues = reinterpret_cast<uint32_t*>(base + w.residues);
+    s.crt_in = reinterpret_cast<uint32_t*>(base + w.crt_in);
+    s.dots = reinterpret_cast<uint64_t*>(base + w.dots);
+    s.result = reinterpret_cast<uint32_t*>(base + w.result);
+    s.error_flag = reinterpret_cast<uint32_t*>(base + w.error_flag);
+    s.convert_engine = s.crt_engine = NEGACYCLIC_GEMM_SIMT;
+    if (!s.gemm_tensor_wanted) return "";
+    std::string why_convert, why_crt;
+    if (prepare_gemm_tensor(s.convert_gemm, reinterpret_cast<const uint8_t*>(s.operands), uint64_t(s.padded_limbs) * 4,
+                            RowMap::split_rows(h.n, h.n_sub, h.split, 0, h.n_sub), 2 * h.n, s.convert_weights,
+                            4 * s.padded_r, s.k_convert, why_convert))
+        s.convert_engine = NEGACYCLIC_GEMM_TENSOR;
+    if (prepare_gemm_tensor(s.crt_gemm, reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4,
+                            RowMap::linear(0), h.n, s.crt_weights, s.crt_columns, s.k_crt, why_crt))
+        s.crt_engine = NEGACYCLIC_GEMM_TENSOR;
+    if (!s.gemm_pairs_allowed) s.convert_gemm.pairs = s.crt_gemm.pairs = false;
+    if (s.gemm_tensor_required &&
+        (s.convert_engine != NEGACYCLIC_GEMM_TENSOR || s.crt_engine != NEGACYCLIC_GEMM_TENSOR))
+        return "tensor-core GEMM not available for this point: " + why_convert + (why_convert.empty() ? "" : "; ") +
+               why_crt;
+    return "";
+}
+
+void enqueue_device_product(negacyclic_plan& s, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
+                            cudaStream_t stream) {
+    launch_pad_operands(d_a, d_b, s.operands, s.host.n, s.host.limbs, s.padded_limbs, stream);
+    enqueue_product(s, d_c, stream);
+}
+
 int cuda_failure(const CudaError& e) {
     return fail(NEGACYCLIC_ECUDA, std::string(e.where) + ": " + cudaGetErrorString(e.code));
 }
 
-struct DeviceGuard {
-    int previous = -1;
-    explicit DeviceGuard(int device) {
-        cudaGetDevice(&previous);
-        if (previous != device) cudaSetDevice(device);
-    }
-    ~DeviceGuard() {
-        if (previous >= 0) cudaSetDevice(previous);
-    }
-};
 
-}  // namespace
+}  // namespace negacyclic::detail
 
 extern "C" {
 
@@ -270,13 +279,13 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         device_alloc(s.crt_weights, size_t(s.crt_columns) * s.k_crt, tables);
         device_alloc(s.q, limbs, tables);
         device_alloc(s.minus_p, limbs, tables);
-        device_alloc(s.crt_words, size_t(s.r) * h.words, work);
-        device_alloc(s.operands, size_t(2) * n * s.padded_limbs, work);
-        device_alloc(s.residues, size_t(2) * s.r * n, work);
-        device_alloc(s.crt_in, size_t(n) * s.padded_r, work);
-        device_alloc(s.dots, size_t(n) * h.words, work);
-        device_alloc(s.result, size_t(n) * limbs, work);
-        device_alloc(s.error_flag, 1, work);
+        device_alloc(s.crt_words, size_t(s.r) * h.words, work);  // freed once the CRT weights are built
+        work = 0;
+        s.work_bytes = work_layout(s).total;
+        if (!o.external_work) {
+            check(cudaMalloc(&s.work_arena, s.work_bytes), "cudaMalloc");
+            work = s.work_bytes;
+        }
         s.table_bytes = tables;
         s.device_bytes = tables + work;
 
@@ -291,29 +300,33 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         check(cudaMemcpyAsync(s.minus_p, h.minus_p_mod_q.data(), limbs * 4, cudaMemcpyHostToDevice, st), "upload");
         check(cudaMemcpyAsync(s.crt_words, h.crt_weights.data(), h.crt_weights.size() * 4, cudaMemcpyHostToDevice, st),
               "upload crt");
-        check(cudaMemsetAsync(s.error_flag, 0, 4, st), "memset");
-        // the K-padding columns of the operands stay zero forever
-        check(cudaMemsetAsync(s.operands, 0, size_t(2) * n * s.padded_limbs * 4, st), "memset");
         launch_twiddles(s.primes, s.r, h.n_sub, s.fwd, s.inv, s.zeta, st);
         launch_convert_weights(s.primes, s.r, s.padded_r, limbs, s.k_convert, s.convert_weights, st);
         launch_crt_weights(s.crt_words, s.r, s.padded_r, h.words, s.crt_columns, s.crt_weights, st);
         check(cudaGetLastError(), "table kernels");
         check(cudaStreamSynchronize(st), "plan tables");
+        cudaFree(s.crt_words);
+        s.crt_words = nullptr;
 
-        if (o.gemm != NEGACYCLIC_GEMM_SIMT) {
-            std::string why_convert, why_crt;
-            if (prepare_gemm_tensor(s.convert_gemm, reinterpret_cast<const uint8_t*>(s.operands),
-                                    uint64_t(s.padded_limbs) * 4, RowMap::split_rows(n, h.n_sub, h.split, 0, h.n_sub), 2 * n,
-                                    s.convert_weights, 4 * s.padded_r, s.k_convert, why_convert))
-                s.convert_engine = NEGACYCLIC_GEMM_TENSOR;
-            if (prepare_gemm_tensor(s.crt_gemm, reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4,
-                                    RowMap::linear(0), n, s.crt_weights, s.crt_columns,
-                                    s.k_crt, why_crt))
-                s.crt_engine = NEGACYCLIC_GEMM_TENSOR;
-            if (o.gemm == NEGACYCLIC_GEMM_TENSOR &&
-                (s.convert_engine != NEGACYCLIC_GEMM_TENSOR || s.crt_engine != NEGACYCLIC_GEMM_TENSOR))
-                return fail(NEGACYCLIC_EINVAL, "tensor-core GEMM not available for this point: " + why_convert +
-                                                   (why_convert.empty() ? "" : "; ") + why_crt);
+        s.gemm_tensor_wanted = o.gemm != NEGACYCLIC_GEMM_SIMT;
+        s.gemm_tensor_required = o.gemm == NEGACYCLIC_GEMM_TENSOR || o.gemm == NEGACYCLIC_GEMM_TENSOR_SINGLE;
+        s.gemm_pairs_allowed = o.gemm != NEGACYCLIC_GEMM_TENSOR_SINGLE;
+        if (s.work_arena) {
+            // padding columns of the operands never reach the product (their conversion weights
+            // are zero), so the arena needs no clearing; zero it anyway for deterministic dumps
+            check(cudaMemsetAsync(s.work_arena, 0, s.work_bytes, st), "memset");
+            check(cudaStreamSynchronize(st), "memset");
+            const std::string why = bind_work(s, s.work_arena);
+            if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
+        } else if (s.gemm_tensor_required) {
+            // check now that the shape takes tensor cores; the real binding comes later
+            void* probe = nullptr;
+            check(cudaMalloc(&probe, 256), "cudaMalloc");
+            const std::string why = bind_work(s, probe);
+            cudaFree(probe);
+            s.operands = s.residues = s.crt_in = s.result = s.error_flag = nullptr;
+            s.dots = nullptr;
+            if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
         }
     } catch (const CudaError& e) {
         cudaGetLastError();
@@ -321,6 +334,30 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
                                                    : cuda_failure(e);
     }
     *out = plan.release();
+    return NEGACYCLIC_OK;
+}
+
+size_t negacyclic_work_bytes(const negacyclic_plan* s) { return s ? s->work_bytes : 0; }
+
+int negacyclic_pipeline_status(uint32_t* flags) {
+    if (!flags) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    *flags = 0;
+    uint32_t* word = tensor_gemm_error_flag();
+    if (!word) return fail(NEGACYCLIC_ECUDA, "cannot read the pipeline status word");
+    if (cudaMemcpy(flags, word, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(word, 0, 4) != cudaSuccess)
+        return fail(NEGACYCLIC_ECUDA, cudaGetErrorString(cudaGetLastError()));
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_bind_work(negacyclic_plan* s, void* d_work, size_t bytes) {
+    if (!s || !d_work) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (s->work_arena) return fail(NEGACYCLIC_EINVAL, "plan owns its work space");
+    if (bytes < s->work_bytes) return fail(NEGACYCLIC_ESIZE, "work space smaller than negacyclic_work_bytes()");
+    if (reinterpret_cast<uintptr_t>(d_work) % 256) return fail(NEGACYCLIC_EINVAL, "work space must be 256-byte aligned");
+    DeviceGuard guard(s->device);
+    const std::string why = bind_work(*s, d_work);
+    if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
     return NEGACYCLIC_OK;
 }
 
@@ -347,11 +384,11 @@ int negacyclic_get_info(const negacyclic_plan* s, negacyclic_info* info) {
 int negacyclic_run_device(negacyclic_plan* s, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                           void* stream_ptr) {
     if (!s || !d_a || !d_b || !d_c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
     DeviceGuard guard(s->device);
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     try {
-        launch_pad_operands(d_a, d_b, s->operands, s->host.n, s->host.limbs, s->padded_limbs, stream);
-        enqueue_product(*s, d_c, stream);
+        enqueue_device_product(*s, d_a, d_b, d_c, stream);
     } catch (const CudaError& e) {
         return cuda_failure(e);
     }
@@ -361,6 +398,7 @@ int negacyclic_run_device(negacyclic_plan* s, const uint32_t* d_a, const uint32_
 int negacyclic_run_device_timed(negacyclic_plan* s, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                                 void* stream_ptr, float* stage_ms) {
     if (!s || !d_a || !d_b || !d_c || !stage_ms) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
     DeviceGuard guard(s->device);
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     cudaEvent_t events[kStages + 2] = {};
@@ -384,12 +422,14 @@ int negacyclic_run_device_timed(negacyclic_plan* s, const uint32_t* d_a, const u
 
 int negacyclic_run(negacyclic_plan* s, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     if (!s || !a || !b || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
     DeviceGuard guard(s->device);
     const HostPlan& h = s->host;
     const size_t row = size_t(h.limbs) * 4, pitch = size_t(s->padded_limbs) * 4;
     const uint32_t chunks = s->chunks, per = h.n / chunks, span = h.n_sub / chunks;
     cudaStream_t st = s->stream;
     try {
+        check(cudaMemsetAsync(s->error_flag, 0, 4, st), "memset");
         // inputs: chunk c's rows of a and b land in the padded operand layout (2-D copies, no pad
         // kernel), then the conversion GEMM of that chunk runs while the next chunk is in flight
         for (uint32_t k = 0; k < chunks; ++k) {

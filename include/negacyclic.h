@@ -45,7 +45,7 @@ extern "C" {
 #define NEGACYCLIC_GEMM_AUTO 0   /* tensor cores where the shape allows it */
 #define NEGACYCLIC_GEMM_SIMT 1   /* dp4a CUDA-core kernel (any shape) */
 #define NEGACYCLIC_GEMM_TENSOR 2 /* tcgen05 kind::i8, TMA-fed, TMEM accumulators (CTA pairs where possible) */
-#define NEGACYCLIC_GEMM_TENSOR_SINGLE 3 /* negacyclic_gemm_u8 only: the single-CTA tcgen05 kernel */
+#define NEGACYCLIC_GEMM_TENSOR_SINGLE 3 /* tcgen05 with single-CTA 128x256 tiles only (no CTA pairs) */
 
 typedef struct negacyclic_plan negacyclic_plan;
 
@@ -53,7 +53,8 @@ typedef struct {
     uint32_t split;     /* ring split s (power of two); 0 = smallest that works */
     uint32_t gemm;      /* NEGACYCLIC_GEMM_* */
     int32_t device;     /* CUDA device ordinal; -1 = the calling thread's current device */
-    uint32_t reserved[5];
+    uint32_t external_work; /* 1: allocate no work space; bind one with negacyclic_bind_work */
+    uint32_t reserved[4];
 } negacyclic_options;
 
 typedef struct {
@@ -111,6 +112,26 @@ int negacyclic_run_device(negacyclic_plan* plan, const uint32_t* d_a, const uint
 int negacyclic_run_device_timed(negacyclic_plan* plan, const uint32_t* d_a, const uint32_t* d_b,
                                 uint32_t* d_c, void* stream, float* stage_ms);
 
+/* Bytes of device work space one product of this plan needs (operands, residues, CRT
+ * inputs and word sums, result). */
+size_t negacyclic_work_bytes(const negacyclic_plan* plan);
+
+/*
+ * Binds a caller-owned, 256-byte-aligned device work space of at least
+ * negacyclic_work_bytes() bytes to a plan created with external_work = 1.
+ * Several plans may share one work space when their products never overlap
+ * in time (same stream); products in flight on different streams need
+ * different work spaces.
+ */
+int negacyclic_bind_work(negacyclic_plan* plan, void* d_work, size_t bytes);
+
+/*
+ * Diagnostics of the current device: *flags receives the tensor-core GEMM status
+ * word (nonzero = a pipeline wait gave up after ~2 s since the last call; bits say
+ * which role) and the word is cleared. Synchronises the device.
+ */
+int negacyclic_pipeline_status(uint32_t* flags);
+
 /* Releases the plan and every device/pinned buffer it holds. NULL is a no-op. */
 void negacyclic_free(negacyclic_plan* plan);
 
@@ -141,6 +162,105 @@ int negacyclic_debug_read(negacyclic_plan* plan, int which, void* host, size_t* 
  */
 int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uint32_t m,
                        uint32_t n, uint32_t k, uint32_t engine, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched form: many products of uneven (N, W, q) in one graph launch.
+ * New in this library (the reference runs one product per harness call,
+ * src/main.cpp:164-204). Instances are planned individually (an autotuner picks
+ * each shape's ring split and GEMM kernel by timing them, cached in a text file),
+ * assigned longest-first to concurrent lanes that share one work arena each,
+ * and captured into a single CUDA graph.
+ */
+typedef struct negacyclic_batch negacyclic_batch;
+
+typedef struct {
+    uint32_t n, w, limbs;  /* as for negacyclic_init */
+    const uint32_t* q;     /* limbs words (read during negacyclic_batch_create only) */
+} negacyclic_point;
+
+typedef struct {
+    uint32_t lanes;          /* concurrent streams; 0 = min(count, 4) */
+    uint32_t tune;           /* 1: time candidate configurations for shapes not in the cache */
+    int32_t device;          /* -1 = current device */
+    uint32_t reserved0;
+    const char* tune_cache;  /* cache file; NULL = $NEGACYCLIC_TUNE_CACHE, or no cache */
+    uint32_t reserved[4];
+} negacyclic_batch_options;
+
+typedef struct {
+    negacyclic_info plan;    /* the instance's plan (split, primes, GEMM engines ...) */
+    uint32_t lane;           /* stream it runs on */
+    uint32_t requested_gemm; /* NEGACYCLIC_GEMM_* chosen by the tuner (0 = default) */
+    double tuned_ms;         /* measured device time of one product (0 = not tuned) */
+} negacyclic_batch_instance;
+
+int negacyclic_batch_create(const negacyclic_point* points, uint32_t count,
+                            const negacyclic_batch_options* opts, negacyclic_batch** batch);
+
+/* Device buffers of instance `index` ([N][L] words each): fill a and b, read c. */
+int negacyclic_batch_io(negacyclic_batch* batch, uint32_t index, uint32_t** d_a, uint32_t** d_b,
+                        uint32_t** d_c);
+
+int negacyclic_batch_get_info(const negacyclic_batch* batch, uint32_t index,
+                              negacyclic_batch_instance* info);
+
+/* Every product of the batch from its device buffers: one cudaGraphLaunch on `stream`. */
+int negacyclic_batch_run_device(negacyclic_batch* batch, void* stream);
+
+/* Instance `index` alone, as one plain product (the per-call path), enqueued on `stream`.
+ * Must not overlap other runs of the same batch (instances share lane work spaces). */
+int negacyclic_batch_run_one(negacyclic_batch* batch, uint32_t index, void* stream);
+
+/* Host arrays a[i], b[i], c[i] per instance; copies overlap other lanes' products. Blocking. */
+int negacyclic_batch_run(negacyclic_batch* batch, const uint32_t* const* a, const uint32_t* const* b,
+                         uint32_t* const* c);
+
+void negacyclic_batch_free(negacyclic_batch* batch);
+
+/* ---------------------------------------------------------------------------
+ * Serving form: a request loop with continuous batching (new in this library).
+ * A session fixes (W, L, q); its plans, one per ring size N, stay resident on
+ * the device. Requests are submitted from any thread and return at once; a
+ * dispatcher admits them in arrival order whenever a stream slot is free and
+ * their device memory fits the HBM budget, so work of requests that arrive
+ * while others run overlaps on the device. Host buffers must stay valid until
+ * negacyclic_server_wait returns; page-locked buffers overlap best.
+ */
+typedef struct negacyclic_server negacyclic_server;
+
+typedef struct {
+    uint64_t hbm_budget;  /* bytes for resident plan tables + in-flight requests; 0 = 60 GiB */
+    uint32_t slots;       /* concurrent requests (streams); 0 = 4 */
+    int32_t device;       /* -1 = current device */
+    uint32_t reserved[4];
+} negacyclic_server_options;
+
+typedef struct {
+    uint64_t completed, failed, queued;
+    uint64_t resident_bytes, in_flight_bytes;
+    double p50_ms, p99_ms, mean_ms;  /* submit -> result on the host, completed requests */
+    double products_per_s;           /* completed / (last finish - first submit) */
+} negacyclic_server_stats;
+
+int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_server** server);
+
+/* Opens a session for (W, L, q); plans for the `count` ring sizes in ns are built now
+ * (others on their first request). */
+int negacyclic_server_open_session(negacyclic_server* server, uint32_t w, uint32_t limbs,
+                                   const uint32_t* q, const uint32_t* ns, uint32_t count,
+                                   uint32_t* session);
+
+int negacyclic_server_submit(negacyclic_server* server, uint32_t session, uint32_t n,
+                             const uint32_t* a, const uint32_t* b, uint32_t* c, uint64_t* request);
+
+/* Blocks until the request finished (or timeout_ms passed; <= 0 waits without limit). */
+int negacyclic_server_wait(negacyclic_server* server, uint64_t request, double timeout_ms,
+                           double* latency_ms);
+
+int negacyclic_server_get_stats(negacyclic_server* server, negacyclic_server_stats* stats);
+
+/* Stops the dispatcher after in-flight work finishes and frees everything. */
+void negacyclic_server_free(negacyclic_server* server);
 
 #ifdef __cplusplus
 }
