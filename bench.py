@@ -373,12 +373,30 @@ def run_batch(args):
         stop.synchronize()
         plain_ms += start.elapsed_time(stop) / max(1, args.steps // 2)
     log(f"plain {plain_ms:.1f} ms per batch, pipeline status {fpc.pipeline_status()}")
+    # host arrays (page-locked): batched (lanes overlap copies with other products) vs one call each
+    pinned = lambda x: torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)  # noqa: E731
+    ha = [pinned(a) for _, _, _, a, _ in instances]
+    hb = [pinned(b) for _, _, _, _, b in instances]
+    hc = [pinned(np.empty_like(a)) for _, _, _, a, _ in instances]
+    batch.run(ha, hb, hc)
+    t1 = time.perf_counter()
+    batch.run(ha, hb, hc)
+    host_batched_ms = (time.perf_counter() - t1) * 1000
+    batch.run(ha, hb, hc, plain=True)
+    t1 = time.perf_counter()
+    batch.run(ha, hb, hc, plain=True)
+    host_plain_ms = (time.perf_counter() - t1) * 1000
+    log(f"host arrays: batched {host_batched_ms:.1f} ms, plain {host_plain_ms:.1f} ms")
     ops = sum(2.0 * (2 * n) * (4 * l) * (4 * batch.info(i)["primes"]) + 2.0 * n * (4 * batch.info(i)["primes"]) *
               (4 * (l + 5)) for i, (n, l, *_r) in enumerate(instances))
     line = {"metric": f"products/s, {len(instances)} uneven products (N in 4096..65536, L log-uniform 32..1747)",
             "value": len(instances) / (batched_ms / 1000), "unit": "products/s", "mode": "batched graph",
             "plain_value": len(instances) / (plain_ms / 1000), "batched_over_plain": plain_ms / batched_ms,
             "ms_per_batch": batched_ms, "plain_ms_per_batch": plain_ms, "int8_tops": ops / (batched_ms / 1000) / 1e12,
+            "host_e2e": {"batched_products_per_s": len(instances) / (host_batched_ms / 1000),
+                         "plain_products_per_s": len(instances) / (host_plain_ms / 1000),
+                         "batched_over_plain": host_plain_ms / host_batched_ms,
+                         "bytes_per_batch": int(sum(3 * a.nbytes for _, _, _, a, _ in instances))},
             "lanes": args.lanes or min(len(instances), 4), "tuned": bool(args.tune), "setup_s": setup_s,
             "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seed 100)"}
     print(json.dumps(line), flush=True)

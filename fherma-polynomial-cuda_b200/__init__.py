@@ -31,9 +31,10 @@ EXPORTED = [
     "negacyclic_last_error", "negacyclic_init", "negacyclic_get_info", "negacyclic_run",
     "negacyclic_run_device", "negacyclic_free", "negacyclic_host_plan", "negacyclic_debug_read",
     "negacyclic_gemm_u8", "negacyclic_run_device_timed", "negacyclic_work_bytes", "negacyclic_bind_work",
-    "negacyclic_pipeline_status",
+    "negacyclic_pipeline_status", "negacyclic_run_begin", "negacyclic_run_finish",
+    "negacyclic_prepare_host",
     "negacyclic_batch_create", "negacyclic_batch_io", "negacyclic_batch_get_info", "negacyclic_batch_run_device",
-    "negacyclic_batch_run", "negacyclic_batch_run_one", "negacyclic_batch_free",
+    "negacyclic_batch_run", "negacyclic_batch_run_one", "negacyclic_batch_run_plain", "negacyclic_batch_free",
     "negacyclic_server_create", "negacyclic_server_open_session", "negacyclic_server_submit",
     "negacyclic_server_wait", "negacyclic_server_get_stats", "negacyclic_server_free",
 ]
@@ -105,6 +106,9 @@ def library() -> ctypes.CDLL:
         lib.negacyclic_work_bytes.restype = ctypes.c_size_t
         lib.negacyclic_bind_work.argtypes = [p, p, ctypes.c_size_t]
         lib.negacyclic_pipeline_status.argtypes = [ctypes.POINTER(u32)]
+        lib.negacyclic_run_begin.argtypes = [p, p, p]
+        lib.negacyclic_run_finish.argtypes = [p, p]
+        lib.negacyclic_prepare_host.argtypes = [p]
         pp = ctypes.POINTER(p)
         lib.negacyclic_batch_create.argtypes = [ctypes.POINTER(PointSpec), u32, ctypes.POINTER(BatchOptions),
                                                 ctypes.POINTER(p)]
@@ -113,6 +117,7 @@ def library() -> ctypes.CDLL:
         lib.negacyclic_batch_run_device.argtypes = [p, p]
         lib.negacyclic_batch_run.argtypes = [p, pp, pp, pp]
         lib.negacyclic_batch_run_one.argtypes = [p, u32, p]
+        lib.negacyclic_batch_run_plain.argtypes = [p, pp, pp, pp]
         lib.negacyclic_batch_free.argtypes = [p]
         lib.negacyclic_batch_free.restype = None
         lib.negacyclic_server_create.argtypes = [ctypes.POINTER(ServerOptions), ctypes.POINTER(p)]
@@ -282,14 +287,15 @@ class Batch:
         """Instance `index` alone on `stream` (the plain per-call path)."""
         _check(library().negacyclic_batch_run_one(self._handle, index, stream), "negacyclic_batch_run_one")
 
-    def run(self, a_list, b_list, c_list=None):
+    def run(self, a_list, b_list, c_list=None, plain: bool = False):
+        """Host arrays in and out; plain=True runs one negacyclic_run per instance instead."""
         a_list = [_u32(a) for a in a_list]
         b_list = [_u32(b) for b in b_list]
         if c_list is None:
             c_list = [np.empty(shape, np.uint32) for shape in self.shapes]
         arr = lambda xs: (ctypes.c_void_p * len(xs))(*[x.ctypes.data for x in xs])  # noqa: E731
-        _check(library().negacyclic_batch_run(self._handle, arr(a_list), arr(b_list), arr(c_list)),
-               "negacyclic_batch_run")
+        fn = library().negacyclic_batch_run_plain if plain else library().negacyclic_batch_run
+        _check(fn(self._handle, arr(a_list), arr(b_list), arr(c_list)), "negacyclic_batch_run")
         return c_list
 
     def close(self):
@@ -379,7 +385,9 @@ class Outputs:
 
 
 def fherma_init(point: Point) -> Plan:
-    return Plan(point.N, point.W, point.L, point.q)
+    plan = Plan(point.N, point.W, point.L, point.q)
+    _check(library().negacyclic_prepare_host(plan.handle), "negacyclic_prepare_host")
+    return plan
 
 
 def fherma_run(state: Plan, inputs: Inputs) -> Outputs:

@@ -379,6 +379,16 @@ int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const ui
     return NEGACYCLIC_OK;
 }
 
+int negacyclic_batch_run_plain(negacyclic_batch* b, const uint32_t* const* a, const uint32_t* const* bb,
+                               uint32_t* const* c) {
+    if (!b || !a || !bb || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    for (uint32_t i = 0; i < b->plans.size(); ++i) {
+        const int status = negacyclic_run(b->plans[i].get(), a[i], bb[i], c[i]);
+        if (status != NEGACYCLIC_OK) return status;
+    }
+    return NEGACYCLIC_OK;
+}
+
 void negacyclic_batch_free(negacyclic_batch* b) { delete b; }
 
 }  // extern "C"

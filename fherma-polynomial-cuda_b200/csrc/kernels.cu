@@ -32,6 +32,21 @@ __global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32
     }
 }
 
+// rows [first, first + count) of both operands: [N][L] (a then b, contiguous) -> [2][N][Lp]
+__global__ void pad_rows_kernel(const uint32_t* __restrict__ staged, uint32_t* __restrict__ out, uint32_t n,
+                                uint32_t limbs, uint32_t padded, uint32_t first, uint32_t count) {
+    const uint64_t per_op = uint64_t(count) * padded;
+    for (uint64_t at = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; at < 2 * per_op;
+         at += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t op = at < per_op ? 0 : 1;
+        const uint64_t within = at - op * per_op;
+        const uint64_t row = first + within / padded;
+        const uint32_t col = uint32_t(within % padded);
+        out[(uint64_t(op) * n + row) * padded + col] =
+            col < limbs ? staged[(uint64_t(op) * n + row) * limbs + col] : 0u;
+    }
+}
+
 __device__ __forceinline__ uint32_t bit_reverse(uint32_t x, uint32_t bits) {
     return bits ? (__brev(x) >> (32 - bits)) : 0u;
 }
@@ -569,6 +584,13 @@ void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, ui
     uint64_t total = 2ull * n * padded_limbs;
     uint32_t blocks = uint32_t(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
     pad_operands_kernel<<<blocks, 256, 0, stream>>>(a, b, out, n, limbs, padded_limbs);
+}
+
+void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
+                     uint32_t first, uint32_t count, cudaStream_t stream) {
+    uint64_t total = 2ull * count * padded_limbs;
+    uint32_t blocks = uint32_t(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+    pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, first, count);
 }
 
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv, uint2* zeta,

@@ -66,6 +66,9 @@ struct Epilogue {
 
 void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n,
                          uint32_t limbs, uint32_t padded_limbs, cudaStream_t stream);
+// rows [first, first + count) of a staged [2][N][L] array into the padded [2][N][Lp] layout
+void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
+                     uint32_t first, uint32_t count, cudaStream_t stream);
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv,
                      uint2* zeta, cudaStream_t stream);
 void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 
 #include "../../include/negacyclic.h"
 #include "gemm_tc.cuh"
@@ -269,6 +270,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         for (uint32_t c = 0; c < s.chunks; ++c) {
             check(cudaEventCreateWithFlags(&s.in_ready[c], cudaEventDisableTiming), "cudaEventCreate");
             check(cudaEventCreateWithFlags(&s.out_ready[c], cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&s.copied_out[c], cudaEventDisableTiming), "cudaEventCreate");
         }
         size_t tables = 0, work = 0;
         device_alloc(s.primes, s.r, tables);
@@ -420,58 +422,158 @@ int negacyclic_run_device_timed(negacyclic_plan* s, const uint32_t* d_a, const u
     return status;
 }
 
+}  // extern "C"
+
+namespace negacyclic::detail {
+
+bool page_locked(const void* ptr) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost || attr.type == cudaMemoryTypeManaged;
+}
+
+// Page-locked staging and the copy team of the host path, made on first use.
+void ensure_staging(negacyclic_plan& s) {
+    const size_t words = size_t(s.host.n) * s.host.limbs;
+    if (!s.stage_in) check(cudaHostAlloc(&s.stage_in, 2 * words * 4, cudaHostAllocWriteCombined), "cudaHostAlloc");
+    if (!s.stage_out) check(cudaHostAlloc(&s.stage_out, words * 4, cudaHostAllocDefault), "cudaHostAlloc");
+    if (!s.team) {
+        const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+        s.team = std::make_unique<CopyTeam>(std::min(8u, hw / 2));
+    }
+}
+
+// Enqueues a host product. Inputs: page-locked arrays go straight to the copy engine,
+// pageable ones through stage_in (the team copies chunk k+1 while chunk k is in flight).
+// Output: straight into c when c is page-locked, else into stage_out for host_finish.
+void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    const HostPlan& h = s.host;
+    const size_t row = size_t(h.limbs) * 4;
+    const uint32_t chunks = s.chunks, per = h.n / chunks, span = h.n_sub / chunks;
+    cudaStream_t st = s.stream;
+    const bool a_locked = page_locked(a), b_locked = page_locked(b);
+    s.outputs_staged = !(c && page_locked(c));
+    if (!a_locked || !b_locked || s.outputs_staged) ensure_staging(s);
+    check(cudaMemsetAsync(s.error_flag, 0, 4, st), "memset");
+    // rows arrive by contiguous copies (pitched copies from pageable memory run row by row),
+    // are padded on the device when L % 4 != 0, and are converted while the next chunk is in
+    // flight. The CRT word-sum buffer, written only after every chunk is converted, stages them.
+    const bool direct = s.padded_limbs == h.limbs;
+    uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
+    const size_t words = size_t(h.n) * h.limbs;
+    for (uint32_t k = 0; k < chunks; ++k) {
+        const size_t first = size_t(k) * per, bytes = size_t(per) * row;
+        const uint32_t* src_a = a + first * h.limbs;
+        const uint32_t* src_b = b + first * h.limbs;
+        if (!a_locked) {
+            s.team->copy(s.stage_in + first * h.limbs, src_a, bytes);
+            src_a = s.stage_in + first * h.limbs;
+        }
+        if (!b_locked) {
+            s.team->copy(s.stage_in + words + first * h.limbs, src_b, bytes);
+            src_b = s.stage_in + words + first * h.limbs;
+        }
+        check(cudaMemcpyAsync(staged + first * h.limbs, src_a, bytes, cudaMemcpyHostToDevice, s.copy_in), "copy a");
+        check(cudaMemcpyAsync(staged + (size_t(h.n) + first) * h.limbs, src_b, bytes, cudaMemcpyHostToDevice,
+                              s.copy_in),
+              "copy b");
+        check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
+        check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
+        if (!direct) launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, uint32_t(first), per, st);
+        enqueue_convert(s, k * span, span, st);
+    }
+    enqueue_middle(s, st, nullptr);
+    // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
+    uint32_t* dst = s.outputs_staged ? s.stage_out : c;
+    for (uint32_t k = 0; k <= chunks; ++k) {
+        if (k < chunks) {
+            enqueue_output(s, k * per, per, s.result, st);
+            check(cudaEventRecord(s.out_ready[k], st), "cudaEventRecord");
+        }
+        if (k >= 1) {
+            const size_t first = size_t(k - 1) * per;
+            check(cudaStreamWaitEvent(s.copy_out, s.out_ready[k - 1], 0), "cudaStreamWaitEvent");
+            check(cudaMemcpyAsync(dst + first * h.limbs, s.result + first * h.limbs, size_t(per) * row,
+                                  cudaMemcpyDeviceToHost, s.copy_out),
+                  "copy c");
+            check(cudaEventRecord(s.copied_out[k - 1], s.copy_out), "cudaEventRecord");
+        }
+    }
+    check(cudaGetLastError(), "product kernels");
+}
+
+// Waits for a host product; copies staged output chunks into c as they land.
+int host_finish(negacyclic_plan& s, uint32_t* c) {
+    const HostPlan& h = s.host;
+    const uint32_t chunks = s.chunks, per = h.n / chunks;
+    if (s.outputs_staged) {
+        for (uint32_t k = 0; k < chunks; ++k) {
+            check(cudaEventSynchronize(s.copied_out[k]), "copy c");
+            const size_t first = size_t(k) * per;
+            s.team->copy(c + first * h.limbs, s.stage_out + first * h.limbs, size_t(per) * h.limbs * 4);
+        }
+    }
+    uint32_t flag = 0, pipeline = 0;
+    check(cudaMemcpyAsync(&flag, s.error_flag, 4, cudaMemcpyDeviceToHost, s.copy_out), "error flag");
+    if (uint32_t* tc = tensor_gemm_error_flag())
+        check(cudaMemcpyAsync(&pipeline, tc, 4, cudaMemcpyDeviceToHost, s.copy_out), "error flag");
+    check(cudaStreamSynchronize(s.copy_out), "product");
+    check(cudaStreamSynchronize(s.stream), "product");
+    if (flag) return fail(NEGACYCLIC_ECUDA, "reduction exceeded its proven correction bound");
+    if (pipeline) return fail(NEGACYCLIC_ECUDA, "tensor-core GEMM pipeline wait timed out");
+    return NEGACYCLIC_OK;
+}
+
+}  // namespace negacyclic::detail
+
+extern "C" {
+
 int negacyclic_run(negacyclic_plan* s, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     if (!s || !a || !b || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
     if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
     DeviceGuard guard(s->device);
-    const HostPlan& h = s->host;
-    const size_t row = size_t(h.limbs) * 4, pitch = size_t(s->padded_limbs) * 4;
-    const uint32_t chunks = s->chunks, per = h.n / chunks, span = h.n_sub / chunks;
-    cudaStream_t st = s->stream;
     try {
-        check(cudaMemsetAsync(s->error_flag, 0, 4, st), "memset");
-        // inputs: chunk c's rows of a and b land in the padded operand layout (2-D copies, no pad
-        // kernel), then the conversion GEMM of that chunk runs while the next chunk is in flight
-        for (uint32_t k = 0; k < chunks; ++k) {
-            const size_t first = size_t(k) * per;
-            check(cudaMemcpy2DAsync(s->operands + first * s->padded_limbs, pitch, a + first * h.limbs, row, row, per,
-                                    cudaMemcpyHostToDevice, s->copy_in),
-                  "copy a");
-            check(cudaMemcpy2DAsync(s->operands + (size_t(h.n) + first) * s->padded_limbs, pitch,
-                                    b + first * h.limbs, row, row, per, cudaMemcpyHostToDevice, s->copy_in),
-                  "copy b");
-            check(cudaEventRecord(s->in_ready[k], s->copy_in), "cudaEventRecord");
-            check(cudaStreamWaitEvent(st, s->in_ready[k], 0), "cudaStreamWaitEvent");
-            enqueue_convert(*s, k * span, span, st);
-        }
-        enqueue_middle(*s, st, nullptr);
-        // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
-        for (uint32_t k = 0; k <= chunks; ++k) {
-            if (k < chunks) {
-                enqueue_output(*s, k * per, per, s->result, st);
-                check(cudaEventRecord(s->out_ready[k], st), "cudaEventRecord");
-            }
-            if (k >= 1) {
-                const size_t first = size_t(k - 1) * per;
-                check(cudaStreamWaitEvent(s->copy_out, s->out_ready[k - 1], 0), "cudaStreamWaitEvent");
-                check(cudaMemcpyAsync(c + first * h.limbs, s->result + first * h.limbs, size_t(per) * row,
-                                      cudaMemcpyDeviceToHost, s->copy_out),
-                      "copy c");
-            }
-        }
-        check(cudaGetLastError(), "product kernels");
-        uint32_t flag = 0, pipeline = 0;
-        check(cudaMemcpyAsync(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost, s->copy_out), "error flag");
-        if (uint32_t* tc = tensor_gemm_error_flag())
-            check(cudaMemcpyAsync(&pipeline, tc, 4, cudaMemcpyDeviceToHost, s->copy_out), "error flag");
-        check(cudaStreamSynchronize(s->copy_out), "product");
-        check(cudaStreamSynchronize(st), "product");
-        if (flag) return fail(NEGACYCLIC_ECUDA, "reduction exceeded its proven correction bound");
-        if (pipeline) return fail(NEGACYCLIC_ECUDA, "tensor-core GEMM pipeline wait timed out");
+        host_begin(*s, a, b, c);
+        return host_finish(*s, c);
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
+}
+
+int negacyclic_prepare_host(negacyclic_plan* s) {
+    if (!s) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    DeviceGuard guard(s->device);
+    try {
+        ensure_staging(*s);
     } catch (const CudaError& e) {
         return cuda_failure(e);
     }
     return NEGACYCLIC_OK;
+}
+
+int negacyclic_run_begin(negacyclic_plan* s, const uint32_t* a, const uint32_t* b) {
+    if (!s || !a || !b) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
+    DeviceGuard guard(s->device);
+    try {
+        host_begin(*s, a, b, nullptr);
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_run_finish(negacyclic_plan* s, uint32_t* c) {
+    if (!s || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    DeviceGuard guard(s->device);
+    try {
+        return host_finish(*s, c);
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
 }
 
 void negacyclic_free(negacyclic_plan* plan) { delete plan; }

@@ -8,7 +8,10 @@
 #include "../../include/negacyclic.h"
 #include "gemm_tc.cuh"
 #include "host_plan.h"
+#include "host_io.h"
 #include "kernels.cuh"
+
+#include <memory>
 
 // The C ABI's opaque plan (include/negacyclic.h).
 struct negacyclic_plan {
@@ -32,6 +35,12 @@ struct negacyclic_plan {
     uint32_t chunks = 1;  // coefficient chunks of the streamed host path
     cudaEvent_t in_ready[kMaxChunks] = {};
     cudaEvent_t out_ready[kMaxChunks] = {};
+    cudaEvent_t copied_out[kMaxChunks] = {};
+    // host path with pageable arrays: page-locked staging and a copy team (made on first use)
+    uint32_t* stage_in = nullptr;   // [2][N][L], write-combined
+    uint32_t* stage_out = nullptr;  // [N][L]
+    std::unique_ptr<negacyclic::CopyTeam> team;
+    bool outputs_staged = false;    // the running host product copies c through stage_out
     size_t device_bytes = 0, table_bytes = 0;
     negacyclic::TensorGemmPlan convert_gemm, crt_gemm;
 
@@ -48,7 +57,11 @@ struct negacyclic_plan {
         for (uint32_t c = 0; c < kMaxChunks; ++c) {
             if (in_ready[c]) cudaEventDestroy(in_ready[c]);
             if (out_ready[c]) cudaEventDestroy(out_ready[c]);
+            if (copied_out[c]) cudaEventDestroy(copied_out[c]);
         }
+        if (stage_in) cudaFreeHost(stage_in);
+        if (stage_out) cudaFreeHost(stage_out);
+        team.reset();
         if (stream) cudaStreamDestroy(stream);
         if (copy_in) cudaStreamDestroy(copy_in);
         if (copy_out) cudaStreamDestroy(copy_out);

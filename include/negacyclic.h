@@ -91,10 +91,27 @@ int negacyclic_get_info(const negacyclic_plan* plan, negacyclic_info* info);
 /*
  * Host-to-host product: a, b, c are host arrays of n*limbs words (c may alias
  * neither input). Copies in, computes, copies out; returns when c is written.
- * Page-locked host memory (cudaHostAlloc / cudaHostRegister) is copied by DMA
- * directly; pageable memory goes through the plan's pinned staging buffers.
+ * Streamed in coefficient chunks: copies of chunk k+1 overlap the conversion of
+ * chunk k on the way in, and the CRT/reduction of chunk k+1 overlaps the copy-out
+ * of chunk k on the way out. Page-locked host memory (cudaHostAlloc /
+ * cudaHostRegister) is read and written by DMA directly; pageable memory goes
+ * through the plan's page-locked staging buffers, filled and drained by a team of
+ * host threads.
  */
 int negacyclic_run(negacyclic_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* c);
+
+/* Allocates now the page-locked staging and host copy threads that negacyclic_run
+ * otherwise makes on its first call with pageable arrays (3 N L words pinned). */
+int negacyclic_prepare_host(negacyclic_plan* plan);
+
+/*
+ * negacyclic_run in two halves, so that a caller can do host work (such as
+ * allocating the output array) while the device computes: begin enqueues
+ * everything with the result staged in page-locked memory; finish waits and
+ * copies it into c. a and b must stay valid until finish returns.
+ */
+int negacyclic_run_begin(negacyclic_plan* plan, const uint32_t* a, const uint32_t* b);
+int negacyclic_run_finish(negacyclic_plan* plan, uint32_t* c);
 
 /*
  * Device-resident product: d_a, d_b, d_c are device arrays of n*limbs words on
@@ -214,6 +231,11 @@ int negacyclic_batch_run_one(negacyclic_batch* batch, uint32_t index, void* stre
 /* Host arrays a[i], b[i], c[i] per instance; copies overlap other lanes' products. Blocking. */
 int negacyclic_batch_run(negacyclic_batch* batch, const uint32_t* const* a, const uint32_t* const* b,
                          uint32_t* const* c);
+
+/* The same host arrays one instance after another through negacyclic_run (the plain
+ * per-call host path), for comparison. Blocking. */
+int negacyclic_batch_run_plain(negacyclic_batch* batch, const uint32_t* const* a,
+                               const uint32_t* const* b, uint32_t* const* c);
 
 void negacyclic_batch_free(negacyclic_batch* batch);
 
