@@ -141,6 +141,23 @@ def distributed():
     return world, rank, local
 
 
+def max_over_ranks(x: float, world: int, device: str = "cpu") -> float:
+    """The slowest rank's time: every rank takes part, every rank gets the maximum."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, steps: int, seconds: float) -> float:
+    """Whole-job products/s of `world` replicas that each ran `steps` products, timed by the slowest."""
+    return world * steps / seconds
+
+
 def run_reference(args):
     """The reference's CPU path (GMP Kronecker, restated) on all host cores."""
     world, rank, _ = distributed()
@@ -202,13 +219,6 @@ def run_b200(args):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # --- device-resident products (clocks sampled from the warm-up through the timed region)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -220,9 +230,9 @@ def run_b200(args):
             plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
         stop.record(stream)
         stop.synchronize()
-    device_ms = max_over_ranks(start.elapsed_time(stop))
+    device_ms = max_over_ranks(start.elapsed_time(stop), world, "cuda")
     barrier()
-    value = world * args.steps / (device_ms / 1000)
+    value = replica_throughput(world, args.steps, device_ms / 1000)
 
     # --- per-stage CUDA-event times over the same number of products (roofline)
     stage_ms = {name: 0.0 for name in fpc.STAGES}
@@ -250,9 +260,9 @@ def run_b200(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         plan.run(ha, hb, out=hc)
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
     barrier()
-    e2e_value = world * args.steps / e2e_s
+    e2e_value = replica_throughput(world, args.steps, e2e_s)
     # the device product must equal the host-path product (both through the C ABI)
     if not np.array_equal(dc.cpu().numpy().view(np.uint32), hc):
         raise RuntimeError("device-resident and host products differ")

@@ -545,9 +545,22 @@ int negacyclic_run(negacyclic_plan* s, const uint32_t* a, const uint32_t* b, uin
 
 int negacyclic_prepare_host(negacyclic_plan* s) {
     if (!s) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    if (!s->operands) return fail(NEGACYCLIC_EINVAL, "no work space bound (negacyclic_bind_work)");
     DeviceGuard guard(s->device);
     try {
         ensure_staging(*s);
+        // warm-up: 0 * 0 through the host path (page-locked inputs, staged output), which
+        // loads every kernel of the path and touches the staging pages once
+        const size_t words = size_t(s->host.n) * s->host.limbs;
+        std::memset(s->stage_in, 0, 2 * words * 4);
+        host_begin(*s, s->stage_in, s->stage_in + words, nullptr);
+        for (uint32_t k = 0; k < s->chunks; ++k) check(cudaEventSynchronize(s->copied_out[k]), "warm-up");
+        check(cudaStreamSynchronize(s->stream), "warm-up");
+        uint32_t flag = 0;
+        check(cudaMemcpy(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost), "warm-up");
+        if (flag) return fail(NEGACYCLIC_ECUDA, "warm-up product reported an error");
+        for (size_t i = 0; i < words; i += 4096)
+            if (s->stage_out[i] != 0) return fail(NEGACYCLIC_ECUDA, "warm-up product of zeros is not zero");
     } catch (const CudaError& e) {
         return cuda_failure(e);
     }

@@ -101,7 +101,10 @@ int negacyclic_get_info(const negacyclic_plan* plan, negacyclic_info* info);
 int negacyclic_run(negacyclic_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* c);
 
 /* Allocates now the page-locked staging and host copy threads that negacyclic_run
- * otherwise makes on its first call with pageable arrays (3 N L words pinned). */
+ * otherwise makes on its first call with pageable arrays (3 N L words pinned), and
+ * runs one product of zero operands through the host path, so that the first real
+ * call does not pay for loading kernels or first use of the staging pages. Depends
+ * on the parameters only. */
 int negacyclic_prepare_host(negacyclic_plan* plan);
 
 /*
