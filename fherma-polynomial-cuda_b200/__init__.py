@@ -32,7 +32,7 @@ EXPORTED = [
     "negacyclic_run_device", "negacyclic_free", "negacyclic_host_plan", "negacyclic_debug_read",
     "negacyclic_gemm_u8", "negacyclic_run_device_timed", "negacyclic_work_bytes", "negacyclic_bind_work",
     "negacyclic_pipeline_status", "negacyclic_run_begin", "negacyclic_run_finish",
-    "negacyclic_prepare_host",
+    "negacyclic_prepare_host", "negacyclic_run_device_static",
     "negacyclic_batch_create", "negacyclic_batch_io", "negacyclic_batch_get_info", "negacyclic_batch_run_device",
     "negacyclic_batch_run", "negacyclic_batch_run_one", "negacyclic_batch_run_plain", "negacyclic_batch_free",
     "negacyclic_server_create", "negacyclic_server_open_session", "negacyclic_server_submit",
@@ -109,6 +109,7 @@ def library() -> ctypes.CDLL:
         lib.negacyclic_run_begin.argtypes = [p, p, p]
         lib.negacyclic_run_finish.argtypes = [p, p]
         lib.negacyclic_prepare_host.argtypes = [p]
+        lib.negacyclic_run_device_static.argtypes = [p, p, p, p, p]
         pp = ctypes.POINTER(p)
         lib.negacyclic_batch_create.argtypes = [ctypes.POINTER(PointSpec), u32, ctypes.POINTER(BatchOptions),
                                                 ctypes.POINTER(p)]
@@ -183,6 +184,12 @@ class Plan:
     def run_device(self, a_ptr: int, b_ptr: int, c_ptr: int, stream: int = 0):
         """Device pointers ([N][L] uint32 each), enqueued on `stream`."""
         _check(library().negacyclic_run_device(self.handle, a_ptr, b_ptr, c_ptr, stream), "negacyclic_run_device")
+
+    def run_device_static(self, a_ptr: int, b_ptr: int, c_ptr: int, stream: int = 0):
+        """run_device with no allocation: the work space is the library's static device array
+        (NEGACYCLIC_STATIC_WORK_BYTES, shared by every such call; order calls on one stream)."""
+        _check(library().negacyclic_run_device_static(self.handle, a_ptr, b_ptr, c_ptr, stream),
+               "negacyclic_run_device_static")
 
     def run_device_timed(self, a_ptr: int, b_ptr: int, c_ptr: int, stream: int = 0) -> dict:
         """run_device, synchronously, returning per-stage milliseconds (CUDA events on `stream`)."""

@@ -146,6 +146,28 @@ size_t negacyclic_work_bytes(const negacyclic_plan* plan);
 int negacyclic_bind_work(negacyclic_plan* plan, void* d_work, size_t bytes);
 
 /*
+ * No counterpart in the reference: an addition of this library for callers that
+ * cannot allocate device memory while they run (cudaFree waits for the whole
+ * device; a framework's allocator may hold nearly all of HBM; a host process may
+ * forbid allocations after start-up).
+ *
+ * negacyclic_run_device without allocation: the same product, enqueued on
+ * `stream`, with the work space in a static device array of
+ * NEGACYCLIC_STATIC_WORK_BYTES that the library keeps on each GPU it runs on.
+ * Make the plan at start-up with external_work = 1 (tables only). Points whose
+ * negacyclic_work_bytes() exceeds the array are rejected (NEGACYCLIC_EINVAL, the
+ * message names both sizes); 64 MiB holds e.g. N = 8192 with L = 128. The plan's
+ * own work-space binding is left as it was.
+ * The first call on a device looks up the array's address (and makes the driver
+ * load it); make that first call before any stream capture. All calls share the
+ * array: calls whose work overlaps on the GPU (other streams, unordered threads)
+ * race and corrupt each other, so order them on one stream or with events.
+ */
+#define NEGACYCLIC_STATIC_WORK_BYTES ((size_t)64 << 20)
+int negacyclic_run_device_static(negacyclic_plan* plan, const uint32_t* d_a, const uint32_t* d_b,
+                                 uint32_t* d_c, void* stream);
+
+/*
  * Diagnostics of the current device: *flags receives the tensor-core GEMM status
  * word (nonzero = a pipeline wait gave up after ~2 s since the last call; bits say
  * which role) and the word is cleared. Synchronises the device.
