@@ -95,15 +95,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
-                                            int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-        "[%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
@@ -160,8 +151,9 @@ __device__ __forceinline__ void tile_coords(uint32_t tile, const TileShape& shap
 }
 
 // Applies the epilogue to 32 accumulator columns (c_base .. c_base+31) of one row.
+// Raw and CRT epilogues of one 32-column chunk of a row (lane = row).
 __device__ __forceinline__ void epilogue_chunk(const Epilogue& epi, const uint32_t (&v)[32], uint32_t c_base,
-                                               uint32_t columns, uint64_t out_row, uint32_t op, uint32_t column) {
+                                               uint32_t columns, uint64_t out_row) {
     if (epi.mode == kEpilogueRaw) {
         int32_t* out = epi.raw + out_row * epi.raw_ld;
 #pragma unroll
@@ -172,16 +164,56 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& epi, const uint32
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
         const uint32_t group_index = c_base / 4 + g;
-        uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
-                     (uint64_t(v[4 * g + 3]) << 24);
-        if (epi.mode == kEpilogueConvert) {
-            if (group_index < epi.r) {
-                const DevicePrime f = epi.primes[group_index];
-                epi.residues[(size_t(op) * epi.r + group_index) * epi.n + column] = redc(s, f.p, f.pinv);
-            }
-        } else if (group_index < epi.words) {
-            epi.dots[out_row * epi.words + group_index] = s;
+        const uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
+                           (uint64_t(v[4 * g + 3]) << 24);
+        if (group_index < epi.words) epi.dots[out_row * epi.words + group_index] = s;
+    }
+}
+
+// One epilogue warp's share of an accumulator: 32 rows (one per lane) x 256 columns starting at
+// col0, read from TMEM at t_base in 32-column chunks.
+// Conversion: column group g = 4k..4k+3 holds the byte dots of prime k; the residue is
+// REDC(sum_d G_d 256^d). The tile's 64 primes are loaded once (lane l: groups l and l + 32)
+// and broadcast by shuffles, instead of one dependent table load per group.
+__device__ __forceinline__ void epilogue_rows(const Epilogue& epi, uint32_t t_base, uint32_t col0, uint32_t columns,
+                                              bool row_ok, uint64_t out_row, uint32_t op, uint32_t column,
+                                              uint32_t lane) {
+    if (epi.mode == kEpilogueConvert) {
+        const uint32_t g0 = col0 / 4;
+        uint32_t p_lo = 1, pinv_lo = 0, p_hi = 1, pinv_hi = 0;
+        if (g0 + lane < epi.r) {
+            p_lo = epi.primes[g0 + lane].p;
+            pinv_lo = epi.primes[g0 + lane].pinv;
         }
+        if (g0 + 32 + lane < epi.r) {
+            p_hi = epi.primes[g0 + 32 + lane].p;
+            pinv_hi = epi.primes[g0 + 32 + lane].pinv;
+        }
+        uint32_t* out = epi.residues + size_t(op) * epi.r * epi.n + column;  // + k * N for prime k
+        for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
+            const uint32_t c_base = col0 + chunk * 32;
+            if (c_base >= columns) break;  // warp-uniform
+            uint32_t v[32];
+            tmem_load32(t_base + chunk * 32, v);
+            const uint32_t from_p = chunk < 4 ? p_lo : p_hi, from_pinv = chunk < 4 ? pinv_lo : pinv_hi;
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                const uint32_t source = (chunk & 3) * 8 + g, k = c_base / 4 + g;
+                const uint32_t p = __shfl_sync(0xffffffffu, from_p, source);
+                const uint32_t pinv = __shfl_sync(0xffffffffu, from_pinv, source);
+                const uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) +
+                                   (uint64_t(v[4 * g + 2]) << 16) + (uint64_t(v[4 * g + 3]) << 24);
+                if (row_ok && k < epi.r) out[size_t(k) * epi.n] = redc(s, p, pinv);
+            }
+        }
+        return;
+    }
+    for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
+        const uint32_t c_base = col0 + chunk * 32;
+        if (c_base >= columns) break;  // warp-uniform
+        uint32_t v[32];
+        tmem_load32(t_base + chunk * 32, v);
+        if (row_ok) epilogue_chunk(epi, v, c_base, columns, out_row);
     }
 }
 
@@ -241,13 +273,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 uint32_t m_tile, n_tile;
                 tile_coords(tile, shape, m_tile, n_tile);
                 const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
-                // A-map coordinates of the tile's first row: (t, op*N' + j) or (0, first + row0)
-                uint32_t a_t = 0, a_row = shape.rows.first + row0;
-                if (shape.rows.mode == kRowsSplit) {
-                    uint32_t op, j;
-                    shape.rows.decompose(row0, op, a_t, j);
-                    a_row = op * shape.rows.n_sub + j;
-                }
+                // operand row of the tile's first row; its 128 rows are consecutive in memory
+                const uint32_t a_row = uint32_t(shape.rows.row(row0));
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kStages, round = step / kStages;
                     if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
@@ -255,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                         break;
                     }
                     mbar_expect_tx(&full[s], kStageBytes);
-                    tma_load_3d(a_smem + s * kATileBytes, &a_map, &full[s], int(ks * kBlockK), int(a_t), int(a_row));
+                    tma_load_2d(a_smem + s * kATileBytes, &a_map, &full[s], int(ks * kBlockK), int(a_row));
                     tma_load_2d(b_smem + s * kBTileBytes, &b_map, &full[s], int(ks * kBlockK), int(col0));
                     issued = step + 1;
                 }
@@ -335,14 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                     out_row = shape.rows.row(row);
             }
             const uint32_t t_base = tmem + acc * kAccColumns + ((quarter * 32) << 16);
-            for (uint32_t chunk = 0; chunk < kBlockN / 32; ++chunk) {
-                const uint32_t c_base = col0 + chunk * 32;
-                if (c_base >= shape.columns) break;  // warp-uniform
-                uint32_t v[32];
-                tmem_load32(t_base + chunk * 32, v);
-                if (!row_ok) continue;
-                epilogue_chunk(epi, v, c_base, shape.columns, out_row, op, column);
-            }
+            epilogue_rows(epi, t_base, col0, shape.columns, row_ok, out_row, op, column, lane);
             // every tcgen05.ld of this warp has completed (tmem_load32 waits): release the accumulator
             fence_before();
             __syncwarp();
@@ -393,15 +413,6 @@ __device__ __forceinline__ uint32_t leader_address(const void* local) {
 
 __device__ __forceinline__ void cluster_sync() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int c0,
-                                                 int c1, int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
-        "%5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
 }
 
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int c0,
@@ -496,12 +507,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 tile_coords(tile, shape, m_tile, n_tile);
                 const uint32_t row0 = m_tile * 256 + rank * kBlockM;
                 const uint32_t col0 = n_tile * kPairBlockN + rank * (kPairBlockN / 2);
-                uint32_t a_t = 0, a_row = shape.rows.first + row0;
-                if (shape.rows.mode == kRowsSplit) {
-                    uint32_t op, j;
-                    shape.rows.decompose(row0, op, a_t, j);
-                    a_row = op * shape.rows.n_sub + j;
-                }
+                const uint32_t a_row = uint32_t(shape.rows.row(row0));  // 128 consecutive operand rows
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kPairStages, round = step / kPairStages;
                     if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
@@ -510,7 +516,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     }
                     if (leader) mbar_expect_tx(&full[s], 2 * kPairStageBytes);
                     const uint32_t bar = leader_address(&full[s]);
-                    tma_load_3d_pair(a_smem + s * kATileBytes, &a_map, bar, int(ks * kBlockK), int(a_t), int(a_row));
+                    tma_load_2d_pair(a_smem + s * kATileBytes, &a_map, bar, int(ks * kBlockK), int(a_row));
                     tma_load_2d_pair(b_smem + s * kPairBTileBytes, &b_map, bar, int(ks * kBlockK), int(col0));
                 }
             }
@@ -587,14 +593,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     out_row = shape.rows.row(row);
             }
             const uint32_t t_base = tmem + acc * kAccColumns + ((quarter * 32) << 16);
-            for (uint32_t chunk = 0; chunk < kPairBlockN / 32; ++chunk) {
-                const uint32_t c_base = col0 + chunk * 32;
-                if (c_base >= shape.columns) break;  // warp-uniform
-                uint32_t v[32];
-                tmem_load32(t_base + chunk * 32, v);
-                if (!row_ok) continue;
-                epilogue_chunk(epi, v, c_base, shape.columns, out_row, op, column);
-            }
+            epilogue_rows(epi, t_base, col0, shape.columns, row_ok, out_row, op, column, lane);
             fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive_cluster(release + acc * sizeof(uint64_t));
@@ -654,9 +653,8 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
         why = "fewer than 256 output columns";
         return false;
     }
-    uint32_t split = 1, slab = m;
+    uint32_t slab = m;
     if (rows.mode == kRowsSplit) {
-        split = rows.split;
         slab = rows.n_sub;
         if (m != 2 * rows.n || rows.first != 0 || rows.span != rows.n_sub) {
             why = "split row map expects both whole operands";
@@ -670,12 +668,13 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
         why = "fewer than 128 rows per transform";
         return false;
     }
-    // A: dims (K bytes, s, rows/s); strides (pitch, s*pitch)
-    const cuuint64_t a_dims[3] = {k_bytes, split, uint64_t(m) / split};
-    const cuuint64_t a_strides[2] = {a_pitch, a_pitch * split};
-    const cuuint32_t a_box[3] = {kBlockK, 1, kBlockM};
-    const cuuint32_t unit[3] = {1, 1, 1};
-    CUresult ra = encode(&plan.a_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(a), a_dims, a_strides,
+    // A: m operand rows of k_bytes (row pitch a_pitch); split-major operands make every
+    // 128-row tile of a split row map one contiguous box
+    const cuuint64_t a_dims[2] = {k_bytes, m};
+    const cuuint64_t a_strides[1] = {a_pitch};
+    const cuuint32_t a_box[2] = {kBlockK, kBlockM};
+    const cuuint32_t unit[2] = {1, 1};
+    CUresult ra = encode(&plan.a_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(a), a_dims, a_strides,
                          a_box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     const cuuint64_t b_dims[2] = {k_bytes, columns};

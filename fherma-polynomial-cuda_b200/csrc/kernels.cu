@@ -1,7 +1,8 @@
 // SIMT stages of the negacyclic product and the parameter-only table builders.
 //
 // Data layout in HBM (one plan, r primes, ring split s, N' = N/s):
-//   operands   [2][N][Lp] u32      a then b, limbs padded to Lp = roundup(L, 4) (16-byte rows)
+//   operands   [2][N][Lp] u32      a then b, limbs padded to Lp = roundup(L, 32) (128-byte rows),
+//                                  split-major: row op*N + t*N' + j holds coefficient s*j + t
 //   residues   [2][r][N]  u32      per (operand, prime): s transforms of N' values,
 //                                  transform t holds coefficients i = s*j + t at j
 //   crt_in     [N][r']    u32      coefficient-major residues v_k (r' = roundup(r, 32))
@@ -18,32 +19,46 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 
-__global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
-                                    uint32_t* __restrict__ out, uint32_t n, uint32_t limbs,
-                                    uint32_t padded) {
-    const uint64_t total = uint64_t(n) * padded;
-    for (uint64_t at = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; at < 2 * total;
-         at += uint64_t(gridDim.x) * blockDim.x) {
-        uint64_t within = at < total ? at : at - total;
-        const uint32_t* src = at < total ? a : b;
-        uint64_t row = within / padded;
-        uint32_t col = uint32_t(within - row * padded);
-        out[at] = col < limbs ? src[row * limbs + col] : 0u;
+// One padded row: Lp words (16-byte aligned) from `limbs` words, zeros above.
+__device__ __forceinline__ void pad_row(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t limbs,
+                                        uint32_t padded, uint32_t lane) {
+    uint4* out = reinterpret_cast<uint4*>(dst);
+    for (uint32_t c = lane; c < padded / 4; c += 32) {
+        const uint32_t w = 4 * c;
+        uint4 v;
+        v.x = w < limbs ? src[w] : 0u;
+        v.y = w + 1 < limbs ? src[w + 1] : 0u;
+        v.z = w + 2 < limbs ? src[w + 2] : 0u;
+        v.w = w + 3 < limbs ? src[w + 3] : 0u;
+        out[c] = v;
     }
 }
 
-// rows [first, first + count) of both operands: [N][L] (a then b, contiguous) -> [2][N][Lp]
+// [N][L] a and b -> [2][N][Lp] split-major: output row op*N + t*N' + j holds coefficient
+// s*j + t of operand op. One warp per output row.
+__global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                    uint32_t* __restrict__ out, uint32_t n, uint32_t limbs, uint32_t padded,
+                                    uint32_t log_split, uint32_t log_n_sub) {
+    const uint32_t lane = threadIdx.x % 32, warps = gridDim.x * (blockDim.x / 32);
+    const uint32_t n_sub_mask = (1u << log_n_sub) - 1;
+    for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < 2 * n; w += warps) {
+        const uint32_t op = w >= n ? 1 : 0, row = w - op * n;
+        const uint32_t i = ((row & n_sub_mask) << log_split) + (row >> log_n_sub);
+        pad_row((op ? b : a) + size_t(i) * limbs, out + size_t(w) * padded, limbs, padded, lane);
+    }
+}
+
+// Coefficients [first, first + count) of both operands from a staged [2][N][L] array into the
+// split-major [2][N][Lp] layout. One warp per coefficient row.
 __global__ void pad_rows_kernel(const uint32_t* __restrict__ staged, uint32_t* __restrict__ out, uint32_t n,
-                                uint32_t limbs, uint32_t padded, uint32_t first, uint32_t count) {
-    const uint64_t per_op = uint64_t(count) * padded;
-    for (uint64_t at = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; at < 2 * per_op;
-         at += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t op = at < per_op ? 0 : 1;
-        const uint64_t within = at - op * per_op;
-        const uint64_t row = first + within / padded;
-        const uint32_t col = uint32_t(within % padded);
-        out[(uint64_t(op) * n + row) * padded + col] =
-            col < limbs ? staged[(uint64_t(op) * n + row) * limbs + col] : 0u;
+                                uint32_t limbs, uint32_t padded, uint32_t log_split, uint32_t log_n_sub,
+                                uint32_t first, uint32_t count) {
+    const uint32_t lane = threadIdx.x % 32, warps = gridDim.x * (blockDim.x / 32);
+    const uint32_t split_mask = (1u << log_split) - 1;
+    for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < 2 * count; w += warps) {
+        const uint32_t op = w >= count ? 1 : 0, i = first + (w - op * count);
+        const uint32_t row = op * n + ((i & split_mask) << log_n_sub) + (i >> log_split);
+        pad_row(staged + (size_t(op) * n + i) * limbs, out + size_t(row) * padded, limbs, padded, lane);
     }
 }
 
@@ -580,17 +595,18 @@ uint32_t log2_u32(uint32_t x) { return x ? 31 - __builtin_clz(x) : 0; }
 }  // namespace
 
 void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, uint32_t limbs,
-                         uint32_t padded_limbs, cudaStream_t stream) {
-    uint64_t total = 2ull * n * padded_limbs;
-    uint32_t blocks = uint32_t(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
-    pad_operands_kernel<<<blocks, 256, 0, stream>>>(a, b, out, n, limbs, padded_limbs);
+                         uint32_t padded_limbs, uint32_t split, cudaStream_t stream) {
+    const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
+    const uint32_t blocks = std::min<uint32_t>((2 * n + 7) / 8, 148 * 16);  // 8 rows (warps) per block
+    pad_operands_kernel<<<blocks, 256, 0, stream>>>(a, b, out, n, limbs, padded_limbs, log_split, log_n_sub);
 }
 
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t first, uint32_t count, cudaStream_t stream) {
-    uint64_t total = 2ull * count * padded_limbs;
-    uint32_t blocks = uint32_t(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
-    pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, first, count);
+                     uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream) {
+    const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
+    const uint32_t blocks = std::min<uint32_t>((2 * count + 7) / 8, 148 * 16);
+    pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, log_split, log_n_sub, first,
+                                                count);
 }
 
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv, uint2* zeta,

@@ -10,8 +10,10 @@ namespace negacyclic {
 // Row addressing of the u8 GEMM's A operand, for one launch (a whole product or a chunk).
 //  kRowsLinear: GEMM row m reads operand row first + m.
 //  kRowsSplit:  GEMM row m = op*(s*span) + t*span + (j - first), j in [first, first+span),
-//               reads coefficient i = s*j + t of operand op (operand row op*N + i) and
-//               produces residue row op, column t*N' + j (transform t, position j).
+//               covers coefficient i = s*j + t of operand op, which the pad kernels store
+//               split-major at operand row op*N + t*N' + j, and produces residue row op,
+//               column t*N' + j (transform t, position j). A (op, t) slab of rows is
+//               contiguous, so every 128-row A tile is one plain 2-D box.
 enum RowMode : int { kRowsLinear = 0, kRowsSplit = 1 };
 
 struct RowMap {
@@ -36,7 +38,7 @@ struct RowMap {
         if (mode == kRowsLinear) return uint64_t(first) + m;
         uint32_t op, t, j;
         decompose(m, op, t, j);
-        return uint64_t(op) * n + uint64_t(j) * split + t;
+        return uint64_t(op) * n + uint64_t(t) * n_sub + j;
     }
     // conversion output position of GEMM row m: residue row `op`, column t*N' + j
     __device__ __forceinline__ void residue(uint32_t m, uint32_t& op, uint32_t& column) const {
@@ -64,11 +66,13 @@ struct Epilogue {
     uint32_t words;
 };
 
+// a, b: [N][L] -> out: [2][N][Lp], rows split-major (coefficient s*j + t at row op*N + t*N' + j),
+// limbs padded with zeros to Lp
 void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n,
-                         uint32_t limbs, uint32_t padded_limbs, cudaStream_t stream);
-// rows [first, first + count) of a staged [2][N][L] array into the padded [2][N][Lp] layout
+                         uint32_t limbs, uint32_t padded_limbs, uint32_t split, cudaStream_t stream);
+// coefficients [first, first + count) of both operands, staged as [2][N][L], into the same layout
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t first, uint32_t count, cudaStream_t stream);
+                     uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream);
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv,
                      uint2* zeta, cudaStream_t stream);
 void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,

@@ -1,7 +1,7 @@
 // C ABI of the exact negacyclic product (include/negacyclic.h).
 //
 // Stage sequence of one product (device-resident; reference stages in brackets):
-//   pad        operands -> [2][N][Lp] (only when L % 4 != 0; the host path pads during H2D)
+//   pad        operands -> [2][N][Lp], split-major rows (the host path pads chunk by chunk)
 //   convert    byte-sliced u8 GEMM + REDC epilogue        [tensor_product<true>, src/solve.cu:88-142]
 //   forward    merged-psi NTT per (operand, prime, t)     [high_stages/middle_stages, src/solve.cu:172-242]
 //   pointwise  s x s products at each evaluation point    [middle_stages, src/solve.cu:227]
@@ -191,7 +191,7 @@ std::string bind_work(negacyclic_plan& s, void* arena) {
 
 void enqueue_device_product(negacyclic_plan& s, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                             cudaStream_t stream) {
-    launch_pad_operands(d_a, d_b, s.operands, s.host.n, s.host.limbs, s.padded_limbs, stream);
+    launch_pad_operands(d_a, d_b, s.operands, s.host.n, s.host.limbs, s.padded_limbs, s.host.split, stream);
     enqueue_product(s, d_c, stream);
 }
 
@@ -257,7 +257,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
     const HostPlan& h = s.host;
     s.r = uint32_t(h.primes.size());
     s.padded_r = round_up(s.r, 32);
-    s.padded_limbs = round_up(limbs, 4);
+    s.padded_limbs = round_up(limbs, 32);  // 128-byte operand rows: each TMA row read is whole L2 lines
     s.k_convert = 4 * s.padded_limbs;
     s.k_crt = 4 * s.padded_r;
     s.crt_columns = round_up(4 * h.words, 64);
@@ -408,7 +408,8 @@ int negacyclic_run_device_timed(negacyclic_plan* s, const uint32_t* d_a, const u
     try {
         for (auto& e : events) check(cudaEventCreate(&e), "cudaEventCreate");
         check(cudaEventRecord(events[0], stream), "cudaEventRecord");
-        launch_pad_operands(d_a, d_b, s->operands, s->host.n, s->host.limbs, s->padded_limbs, stream);
+        launch_pad_operands(d_a, d_b, s->operands, s->host.n, s->host.limbs, s->padded_limbs, s->host.split,
+                            stream);
         check(cudaEventRecord(events[1], stream), "cudaEventRecord");
         enqueue_product(*s, d_c, stream, events + 2);
         check(cudaEventSynchronize(events[kStages + 1]), "product");
@@ -459,9 +460,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     if (!a_locked || !b_locked || s.outputs_staged) ensure_staging(s);
     check(cudaMemsetAsync(s.error_flag, 0, 4, st), "memset");
     // rows arrive by contiguous copies (pitched copies from pageable memory run row by row),
-    // are padded on the device when L % 4 != 0, and are converted while the next chunk is in
-    // flight. The CRT word-sum buffer, written only after every chunk is converted, stages them.
-    const bool direct = s.padded_limbs == h.limbs;
+    // are padded and put in split-major order on the device unless they already land in place
+    // (L % 4 == 0 and s == 1), and are converted while the next chunk is in flight. The CRT
+    // word-sum buffer, written only after every chunk is converted, stages them.
+    const bool direct = s.padded_limbs == h.limbs && h.split == 1;
     uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
     const size_t words = size_t(h.n) * h.limbs;
     for (uint32_t k = 0; k < chunks; ++k) {
@@ -482,7 +484,8 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
               "copy b");
         check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
         check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
-        if (!direct) launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, uint32_t(first), per, st);
+        if (!direct)
+            launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, h.split, uint32_t(first), per, st);
         enqueue_convert(s, k * span, span, st);
     }
     enqueue_middle(s, st, nullptr);
