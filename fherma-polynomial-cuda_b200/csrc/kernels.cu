@@ -247,44 +247,51 @@ constexpr uint32_t kPerThread = 16;
 
 __device__ __forceinline__ uint32_t padded(uint32_t i) { return i + (i >> 5); }  // bank-conflict padding
 
-// Cooley-Tukey stages with half-sizes t_min*2^(R-1) .. t_min (forward, merged psi twiddles).
+// Cooley-Tukey stages with half-sizes t_min*2^(R-1) .. t_min (forward, merged psi twiddles) on
+// one group of 2^R values. With j = base + k*t_min and base = group_hi * 2^(log t_min + R) + off
+// (off < t_min), butterfly (k, k + half) of stage r has twiddle m + (j >> (log t + 1))
+// = m + group_hi * 2^r + (k >> (R - r)): the 2^(R-1-r) butterflies of block b = k >> (R - r)
+// share one twiddle, so a pass loads 2^R - 1 twiddles for its R * 2^(R-1) butterflies.
 template <int R>
-__device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t base, uint32_t log_t_min, uint32_t log_n,
-                                          const uint2* __restrict__ table, uint32_t p) {
+__device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t group_hi, uint32_t log_t_min,
+                                          uint32_t log_n, const uint2* __restrict__ table, uint32_t p) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int half = 1 << (R - 1 - r);
         const uint32_t log_t = log_t_min + (R - 1 - r);  // this stage's half-size t = 2^log_t
         const uint32_t m = 1u << (log_n - 1 - log_t);     // number of groups: n / (2t)
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-            if (k & half) continue;
-            const uint32_t j = base + (uint32_t(k) << log_t_min);
-            const uint2 w = __ldg(&table[m + (j >> (log_t + 1))]);
-            const uint32_t u = x[k], v = shoup(x[k + half], w.x, w.y, p);
-            x[k] = add_mod(u, v, p);
-            x[k + half] = sub_mod(u, v, p);
+        for (int b = 0; b < (1 << r); ++b) {
+            const uint2 w = __ldg(&table[m + (group_hi << r) + b]);
+#pragma unroll
+            for (int k = b * 2 * half; k < b * 2 * half + half; ++k) {
+                const uint32_t u = x[k], v = shoup(x[k + half], w.x, w.y, p);
+                x[k] = add_mod(u, v, p);
+                x[k + half] = sub_mod(u, v, p);
+            }
         }
     }
 }
 
-// Gentleman-Sande stages with half-sizes t_min .. t_min*2^(R-1) (inverse).
+// Gentleman-Sande stages with half-sizes t_min .. t_min*2^(R-1) (inverse). Stage r's butterflies
+// (k, k + 2^r) in block b = k >> (r + 1) share twiddle h + group_hi * 2^(R-1-r) + b.
 template <int R>
-__device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t base, uint32_t log_t_min, uint32_t log_n,
-                                          const uint2* __restrict__ table, uint32_t p) {
+__device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t group_hi, uint32_t log_t_min,
+                                          uint32_t log_n, const uint2* __restrict__ table, uint32_t p) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int half = 1 << r;
         const uint32_t log_t = log_t_min + r;
         const uint32_t h = 1u << (log_n - 1 - log_t);
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-            if (k & half) continue;
-            const uint32_t j = base + (uint32_t(k) << log_t_min);
-            const uint2 w = __ldg(&table[h + (j >> (log_t + 1))]);
-            const uint32_t u = x[k], v = x[k + half];
-            x[k] = add_mod(u, v, p);
-            x[k + half] = shoup(sub_mod(u, v, p), w.x, w.y, p);
+        for (int b = 0; b < (1 << (R - 1 - r)); ++b) {
+            const uint2 w = __ldg(&table[h + (group_hi << (R - 1 - r)) + b]);
+#pragma unroll
+            for (int k = b * 2 * half; k < b * 2 * half + half; ++k) {
+                const uint32_t u = x[k], v = x[k + half];
+                x[k] = add_mod(u, v, p);
+                x[k + half] = shoup(sub_mod(u, v, p), w.x, w.y, p);
+            }
         }
     }
 }
@@ -302,31 +309,53 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
         const uint32_t group = threadIdx.x + g * kThreads;
         const uint32_t off = group & ((1u << kLogTMin) - 1);
         const uint32_t base = ((group >> kLogTMin) << (kLogTMin + R)) + off;
+        // with t_min = 1 a group is 2^R consecutive words (base a multiple of 2^R): global
+        // accesses go four words at a time, so a warp instruction covers 16-byte pieces
+        constexpr bool kVector = kLogTMin == 0 && R >= 2;
         uint32_t x[1 << R];
+        if constexpr (kFromGlobal && kVector) {
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-            const uint32_t i = base + (uint32_t(k) << kLogTMin);
-            x[k] = kFromGlobal ? src[i] : src[padded(i)];
+            for (int q = 0; q < (1 << R) / 4; ++q) {
+                const uint4 w = reinterpret_cast<const uint4*>(src + base)[q];
+                x[4 * q] = w.x;
+                x[4 * q + 1] = w.y;
+                x[4 * q + 2] = w.z;
+                x[4 * q + 3] = w.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < (1 << R); ++k) {
+                const uint32_t i = base + (uint32_t(k) << kLogTMin);
+                x[k] = kFromGlobal ? src[i] : src[padded(i)];
+            }
         }
         if (kForward)
-            ct_stages<R>(x, base, kLogTMin, kLog, table, p);
+            ct_stages<R>(x, group >> kLogTMin, kLogTMin, kLog, table, p);
         else
-            gs_stages<R>(x, base, kLogTMin, kLog, table, p);
+            gs_stages<R>(x, group >> kLogTMin, kLogTMin, kLog, table, p);
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-            const uint32_t i = base + (uint32_t(k) << kLogTMin);
-            uint32_t value = x[k];
-            if (kScale) value = shoup(value, f, f_q, p);
-            if (kToGlobal)
-                dst[i] = value;
-            else
-                dst[padded(i)] = value;
+        for (int k = 0; k < (1 << R); ++k)
+            if (kScale) x[k] = shoup(x[k], f, f_q, p);
+        if constexpr (kToGlobal && kVector) {
+#pragma unroll
+            for (int q = 0; q < (1 << R) / 4; ++q)
+                reinterpret_cast<uint4*>(dst + base)[q] = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < (1 << R); ++k) {
+                const uint32_t i = base + (uint32_t(k) << kLogTMin);
+                if (kToGlobal)
+                    dst[i] = x[k];
+                else
+                    dst[padded(i)] = x[k];
+            }
         }
     }
 }
 
 // Passes kDone.. of a length-2^kLog transform: four stages per pass, the remainder last.
-// Forward runs half-sizes large -> small; inverse small -> large and scales its output.
+// Forward runs half-sizes large -> small (its short last pass keeps the global stores of
+// consecutive words narrow per thread); inverse small -> large and scales its output.
 template <bool kForward, uint32_t kLog, uint32_t kDone>
 __device__ __forceinline__ void ntt_passes(uint32_t* data, uint32_t* xs, const uint2* __restrict__ table, uint32_t p,
                                            uint32_t f, uint32_t f_q) {
