@@ -656,7 +656,8 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     uint32_t slab = m;
     if (rows.mode == kRowsSplit) {
         slab = rows.n_sub;
-        if (m != 2 * rows.n || rows.first != 0 || rows.span != rows.n_sub) {
+        if (m != 2 * rows.n || rows.first != 0 || rows.span != rows.n_sub || rows.t_first != 0 ||
+            rows.t_count != rows.split) {
             why = "split row map expects both whole operands";
             return false;
         }
@@ -724,7 +725,7 @@ bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_
     if (!plan.ready || rows.mode != plan.rows.mode) return false;
     if (rows.mode == kRowsSplit)
         return rows.span % kBlockM == 0 && rows.first % kBlockM == 0 && rows.first + rows.span <= plan.rows.n_sub &&
-               m == 2 * rows.split * rows.span;
+               rows.t_first + rows.t_count <= plan.rows.split && m == 2 * rows.t_count * rows.span;
     return uint64_t(rows.first) + m <= plan.m;
 }
 

@@ -39,17 +39,36 @@ public:
     CopyTeam& operator=(const CopyTeam&) = delete;
 
     // dst[0..bytes) = src[0..bytes), split over the workers and the calling thread.
-    void copy(void* dst, const void* src, size_t bytes) {
+    void copy(void* dst, const void* src, size_t bytes) { run(dst, src, 0, 0, bytes, 1); }
+
+    // `rows` rows of row_bytes each, from src (rows src_stride bytes apart) to dst (rows
+    // dst_stride bytes apart), split by rows over the workers and the calling thread.
+    void copy_rows(void* dst, size_t dst_stride, const void* src, size_t src_stride, size_t row_bytes,
+                   size_t rows) {
+        if (rows == 1) {
+            copy(dst, src, row_bytes);
+            return;
+        }
+        run(dst, src, dst_stride, src_stride, row_bytes, rows);
+    }
+
+private:
+    void run(void* dst, const void* src, size_t dst_stride, size_t src_stride, size_t row_bytes, size_t rows) {
         const unsigned parts = unsigned(threads_.size()) + 1;
-        if (bytes < (size_t(1) << 20) || parts == 1) {
-            std::memcpy(dst, src, bytes);
+        if (row_bytes * rows < (size_t(1) << 20) || parts == 1) {
+            for (size_t i = 0; i < rows; ++i)
+                std::memcpy(static_cast<char*>(dst) + i * dst_stride, static_cast<const char*>(src) + i * src_stride,
+                            row_bytes);
             return;
         }
         {
             std::lock_guard<std::mutex> lock(mu_);
             dst_ = static_cast<char*>(dst);
             src_ = static_cast<const char*>(src);
-            bytes_ = bytes;
+            dst_stride_ = dst_stride;
+            src_stride_ = src_stride;
+            bytes_ = row_bytes;
+            rows_ = rows;
             parts_ = parts;
             pending_ = parts - 1;
             ++generation_;
@@ -60,8 +79,12 @@ public:
         done_.wait(lock, [this] { return pending_ == 0; });
     }
 
-private:
     void slice(unsigned index) {
+        if (rows_ > 1) {  // whole rows per part
+            const size_t begin = rows_ * index / parts_, end = rows_ * (index + 1) / parts_;
+            for (size_t i = begin; i < end; ++i) std::memcpy(dst_ + i * dst_stride_, src_ + i * src_stride_, bytes_);
+            return;
+        }
         const size_t step = (bytes_ / parts_ + 63) / 64 * 64;
         const size_t begin = std::min(bytes_, step * index), end = std::min(bytes_, begin + step);
         if (index + 1 == parts_) {  // the last slice takes the remainder
@@ -95,7 +118,7 @@ private:
     bool stop_ = false;
     char* dst_ = nullptr;
     const char* src_ = nullptr;
-    size_t bytes_ = 0;
+    size_t dst_stride_ = 0, src_stride_ = 0, bytes_ = 0, rows_ = 1;
     unsigned parts_ = 1, pending_ = 0;
 };
 

@@ -48,8 +48,10 @@ __global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32
     }
 }
 
-// Coefficients [first, first + count) of both operands from a staged [2][N][L] array into the
-// split-major [2][N][Lp] layout. One warp per coefficient row.
+// Rows [first, first + count) of both operands (operand stride N rows) from an unpadded [2][N][L]
+// array into the padded split-major layout. Staged rows are either already split-major
+// (log_split = 0: row = position) or in coefficient order (row i goes to t*N' + j, i = s*j + t).
+// One warp per row.
 __global__ void pad_rows_kernel(const uint32_t* __restrict__ staged, uint32_t* __restrict__ out, uint32_t n,
                                 uint32_t limbs, uint32_t padded, uint32_t log_split, uint32_t log_n_sub,
                                 uint32_t first, uint32_t count) {
@@ -57,8 +59,8 @@ __global__ void pad_rows_kernel(const uint32_t* __restrict__ staged, uint32_t* _
     const uint32_t split_mask = (1u << log_split) - 1;
     for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < 2 * count; w += warps) {
         const uint32_t op = w >= count ? 1 : 0, i = first + (w - op * count);
-        const uint32_t row = op * n + ((i & split_mask) << log_n_sub) + (i >> log_split);
-        pad_row(staged + (size_t(op) * n + i) * limbs, out + size_t(row) * padded, limbs, padded, lane);
+        const uint32_t row = ((i & split_mask) << log_n_sub) + (i >> log_split);
+        pad_row(staged + (size_t(op) * n + i) * limbs, out + (size_t(op) * n + row) * padded, limbs, padded, lane);
     }
 }
 
@@ -190,9 +192,9 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restric
 
 __global__ void __launch_bounds__(512) ntt_forward_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
                                                           const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
-                                                          uint32_t n_sub) {
+                                                          uint32_t n_sub, uint32_t t_first) {
     extern __shared__ uint32_t x[];
-    const uint32_t t_index = blockIdx.x, k = blockIdx.y, op = blockIdx.z;
+    const uint32_t t_index = t_first + blockIdx.x, k = blockIdx.y, op = blockIdx.z;
     const uint32_t p = primes[k].p;
     uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * n_sub;
     const uint2* table = fwd + size_t(k) * n_sub;
@@ -214,9 +216,9 @@ __global__ void __launch_bounds__(512) ntt_forward_kernel(uint32_t* residues, co
 
 __global__ void __launch_bounds__(512) ntt_inverse_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
                                                           const uint2* __restrict__ inv, uint32_t r, uint32_t n,
-                                                          uint32_t n_sub) {
+                                                          uint32_t n_sub, uint32_t v_first) {
     extern __shared__ uint32_t x[];
-    const uint32_t v_index = blockIdx.x, k = blockIdx.y;
+    const uint32_t v_index = v_first + blockIdx.x, k = blockIdx.y;
     const DevicePrime f = primes[k];
     uint32_t* data = residues + size_t(k) * n + size_t(v_index) * n_sub;
     const uint2* table = inv + size_t(k) * n_sub;
@@ -370,14 +372,15 @@ __device__ __forceinline__ void ntt_passes(uint32_t* data, uint32_t* xs, const u
     }
 }
 
-// grid (2s, r): x = op*s + t, y = prime, so a prime's 2s transforms share its twiddles in L2
+// grid (2 t_count, r): x = op*t_count + (t - t_first), y = prime, so a prime's transforms
+// share its twiddles in L2
 template <uint32_t kLog>
 __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_forward_blocked_kernel(
     uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
-    uint32_t split) {
+    uint32_t t_first, uint32_t t_count) {
     extern __shared__ uint32_t xs[];
     constexpr uint32_t kN = 1u << kLog;
-    const uint32_t op = blockIdx.x / split, t_index = blockIdx.x - op * split, k = blockIdx.y;
+    const uint32_t op = blockIdx.x / t_count, t_index = t_first + blockIdx.x - op * t_count, k = blockIdx.y;
     uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * kN;
     ntt_passes<true, kLog, 0>(data, xs, fwd + size_t(k) * kN, primes[k].p, 0, 0);
 }
@@ -385,10 +388,10 @@ __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_fo
 template <uint32_t kLog>
 __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_inverse_blocked_kernel(
     uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ inv, uint32_t r, uint32_t n,
-    uint32_t split) {
+    uint32_t v_first, uint32_t v_count) {
     extern __shared__ uint32_t xs[];
     constexpr uint32_t kN = 1u << kLog;
-    const uint32_t v_index = blockIdx.x, k = blockIdx.y;
+    const uint32_t v_index = v_first + blockIdx.x, k = blockIdx.y;
     const DevicePrime f = primes[k];
     uint32_t* data = residues + size_t(k) * n + size_t(v_index) * kN;
     ntt_passes<false, kLog, 0>(data, xs, inv + size_t(k) * kN, f.p, f.finish, f.finish_q);
@@ -432,22 +435,24 @@ __global__ void pointwise_kernel(uint32_t* residues, const DevicePrime* __restri
     }
 }
 
-// residues[0][k][t*N'+j] -> crt_in[s*j+t][k]; zero for k in [r, r').
+// residues[0][k][rho] -> crt_in[s*j + v][k] for rho = v*N' + j in [first, first + count) (coefficient
+// s*j + v, coefficient-major); zero for k in [r, r').
 __global__ void transpose_kernel(const uint32_t* __restrict__ residues, uint32_t* __restrict__ crt_in,
-                                 uint32_t r, uint32_t padded_r, uint32_t n, uint32_t n_sub, uint32_t split) {
+                                 uint32_t r, uint32_t padded_r, uint32_t n, uint32_t log_split, uint32_t log_n_sub,
+                                 uint32_t first, uint32_t count) {
     __shared__ uint32_t tile[32][33];
-    const uint32_t rho0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-    const uint32_t x = threadIdx.x, y = threadIdx.y;
+    const uint32_t rho0 = first + blockIdx.x * 32, k0 = blockIdx.y * 32, end = first + count;
+    const uint32_t x = threadIdx.x, y = threadIdx.y, n_sub_mask = (1u << log_n_sub) - 1;
     for (uint32_t dy = 0; dy < 32; dy += 8) {
         uint32_t k = k0 + y + dy, rho = rho0 + x;
-        tile[y + dy][x] = (k < r && rho < n) ? residues[size_t(k) * n + rho] : 0u;
+        tile[y + dy][x] = (k < r && rho < end) ? residues[size_t(k) * n + rho] : 0u;
     }
     __syncthreads();
     for (uint32_t dy = 0; dy < 32; dy += 8) {
         uint32_t rho = rho0 + y + dy, k = k0 + x;
-        if (rho >= n || k >= padded_r) continue;
-        uint32_t t = rho / n_sub, j = rho - t * n_sub;
-        crt_in[(size_t(j) * split + t) * padded_r + k] = tile[x][y + dy];
+        if (rho >= end || k >= padded_r) continue;
+        const size_t coefficient = (size_t(rho & n_sub_mask) << log_split) + (rho >> log_n_sub);
+        crt_in[coefficient * padded_r + k] = tile[x][y + dy];
     }
 }
 
@@ -631,10 +636,10 @@ void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, ui
 }
 
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream) {
+                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream) {
     const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
     const uint32_t blocks = std::min<uint32_t>((2 * count + 7) / 8, 148 * 16);
-    pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, log_split, log_n_sub, first,
+    pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, log_split, log_n_sub, first_row,
                                                 count);
 }
 
@@ -669,7 +674,7 @@ static uint32_t ntt_threads(uint32_t n_sub) {
 
 template <bool kForward, uint32_t kLog>
 static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const uint2* table, uint32_t r, uint32_t n,
-                           uint32_t split, cudaStream_t stream) {
+                           uint32_t first, uint32_t count, cudaStream_t stream) {
     constexpr uint32_t kN = 1u << kLog;
     const size_t smem = (kN + kN / 32) * sizeof(uint32_t);
     auto kernel = kForward ? ntt_forward_blocked_kernel<kLog> : ntt_inverse_blocked_kernel<kLog>;
@@ -678,38 +683,38 @@ static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const 
         cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         configured = true;
     }
-    dim3 grid(kForward ? 2 * split : split, r);
-    kernel<<<grid, kN / kPerThread, smem, stream>>>(residues, primes, table, r, n, split);
+    dim3 grid(kForward ? 2 * count : count, r);
+    kernel<<<grid, kN / kPerThread, smem, stream>>>(residues, primes, table, r, n, first, count);
 }
 
 template <bool kForward>
 static bool launch_blocked_any(uint32_t n_sub, uint32_t* residues, const DevicePrime* primes, const uint2* table,
-                               uint32_t r, uint32_t n, uint32_t split, cudaStream_t stream) {
+                               uint32_t r, uint32_t n, uint32_t first, uint32_t count, cudaStream_t stream) {
     switch (n_sub) {
-        case 256: launch_blocked<kForward, 8>(residues, primes, table, r, n, split, stream); return true;
-        case 512: launch_blocked<kForward, 9>(residues, primes, table, r, n, split, stream); return true;
-        case 1024: launch_blocked<kForward, 10>(residues, primes, table, r, n, split, stream); return true;
-        case 2048: launch_blocked<kForward, 11>(residues, primes, table, r, n, split, stream); return true;
-        case 4096: launch_blocked<kForward, 12>(residues, primes, table, r, n, split, stream); return true;
-        case 8192: launch_blocked<kForward, 13>(residues, primes, table, r, n, split, stream); return true;
+        case 256: launch_blocked<kForward, 8>(residues, primes, table, r, n, first, count, stream); return true;
+        case 512: launch_blocked<kForward, 9>(residues, primes, table, r, n, first, count, stream); return true;
+        case 1024: launch_blocked<kForward, 10>(residues, primes, table, r, n, first, count, stream); return true;
+        case 2048: launch_blocked<kForward, 11>(residues, primes, table, r, n, first, count, stream); return true;
+        case 4096: launch_blocked<kForward, 12>(residues, primes, table, r, n, first, count, stream); return true;
+        case 8192: launch_blocked<kForward, 13>(residues, primes, table, r, n, first, count, stream); return true;
         default: return false;
     }
 }
 
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r, uint32_t n,
-                        uint32_t n_sub, uint32_t split, cudaStream_t stream) {
-    if (launch_blocked_any<true>(n_sub, residues, primes, fwd, r, n, split, stream)) return;
-    dim3 grid(split, r, 2);
+                        uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream) {
+    if (launch_blocked_any<true>(n_sub, residues, primes, fwd, r, n, t_first, t_count, stream)) return;
+    dim3 grid(t_count, r, 2);
     ntt_forward_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, fwd, r, n,
-                                                                                          n_sub);
+                                                                                          n_sub, t_first);
 }
 
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r, uint32_t n,
-                        uint32_t n_sub, uint32_t split, cudaStream_t stream) {
-    if (launch_blocked_any<false>(n_sub, residues, primes, inv, r, n, split, stream)) return;
-    dim3 grid(split, r);
+                        uint32_t n_sub, uint32_t v_first, uint32_t v_count, cudaStream_t stream) {
+    if (launch_blocked_any<false>(n_sub, residues, primes, inv, r, n, v_first, v_count, stream)) return;
+    dim3 grid(v_count, r);
     ntt_inverse_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, inv, r, n,
-                                                                                          n_sub);
+                                                                                          n_sub, v_first);
 }
 
 void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r, uint32_t n,
@@ -725,9 +730,11 @@ void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2
 }
 
 void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r, uint32_t n,
-                      uint32_t n_sub, uint32_t split, cudaStream_t stream) {
-    dim3 grid((n + 31) / 32, padded_r / 32);
-    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, n_sub, split);
+                      uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream) {
+    const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
+    dim3 grid((count + 31) / 32, padded_r / 32);
+    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, log_split, log_n_sub, first,
+                                                       count);
 }
 
 void launch_reduce(const ReduceParams& params, cudaStream_t stream) {

@@ -9,8 +9,9 @@ namespace negacyclic {
 
 // Row addressing of the u8 GEMM's A operand, for one launch (a whole product or a chunk).
 //  kRowsLinear: GEMM row m reads operand row first + m.
-//  kRowsSplit:  GEMM row m = op*(s*span) + t*span + (j - first), j in [first, first+span),
-//               covers coefficient i = s*j + t of operand op, which the pad kernels store
+//  kRowsSplit:  GEMM row m = op*(t_count*span) + (t - t_first)*span + (j - first),
+//               t in [t_first, t_first + t_count), j in [first, first + span), covers
+//               coefficient i = s*j + t of operand op, which the pad kernels store
 //               split-major at operand row op*N + t*N' + j, and produces residue row op,
 //               column t*N' + j (transform t, position j). A (op, t) slab of rows is
 //               contiguous, so every 128-row A tile is one plain 2-D box.
@@ -19,19 +20,23 @@ enum RowMode : int { kRowsLinear = 0, kRowsSplit = 1 };
 struct RowMap {
     int mode;
     uint32_t n, n_sub, split;
-    uint32_t first;  // linear: first operand row; split: first j
-    uint32_t span;   // split: j values per (operand, t) in this launch
+    uint32_t first;    // linear: first operand row; split: first j
+    uint32_t span;     // split: j values per (operand, t) in this launch
+    uint32_t t_first;  // split: transforms [t_first, t_first + t_count) in this launch
+    uint32_t t_count;
 
-    static RowMap linear(uint32_t first_row) { return RowMap{kRowsLinear, 0, 0, 1, first_row, 0}; }
-    static RowMap split_rows(uint32_t n, uint32_t n_sub, uint32_t split, uint32_t first_j, uint32_t j_span) {
-        return RowMap{kRowsSplit, n, n_sub, split, first_j, j_span};
+    static RowMap linear(uint32_t first_row) { return RowMap{kRowsLinear, 0, 0, 1, first_row, 0, 0, 1}; }
+    static RowMap split_rows(uint32_t n, uint32_t n_sub, uint32_t split, uint32_t first_j, uint32_t j_span,
+                             uint32_t t_first, uint32_t t_count) {
+        return RowMap{kRowsSplit, n, n_sub, split, first_j, j_span, t_first, t_count};
     }
     __host__ __device__ __forceinline__ void decompose(uint32_t m, uint32_t& op, uint32_t& t, uint32_t& j) const {
-        const uint32_t per_op = split * span;
+        const uint32_t per_op = t_count * span;
         op = m / per_op;
         const uint32_t rem = m - op * per_op;
-        t = rem / span;
-        j = first + (rem - t * span);
+        const uint32_t dt = rem / span;
+        t = t_first + dt;
+        j = first + (rem - dt * span);
     }
     // operand row read by GEMM row m
     __device__ __forceinline__ uint64_t row(uint32_t m) const {
@@ -70,9 +75,11 @@ struct Epilogue {
 // limbs padded with zeros to Lp
 void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n,
                          uint32_t limbs, uint32_t padded_limbs, uint32_t split, cudaStream_t stream);
-// coefficients [first, first + count) of both operands, staged as [2][N][L], into the same layout
+// rows [first_row, first_row + count) of both operands (operand stride N rows) from an unpadded
+// [2][N][L] array into the padded split-major [2][N][Lp] layout: staged in coefficient order
+// (split = s, rows are permuted) or already split-major (split = 1)
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream);
+                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream);
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv,
                      uint2* zeta, cudaStream_t stream);
 void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,
@@ -81,18 +88,22 @@ void launch_crt_weights(const uint32_t* weights_words, uint32_t r, uint32_t padd
                         uint32_t columns, uint8_t* out, cudaStream_t stream);
 void launch_gemm_simt(const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m, const uint8_t* b,
                       uint32_t columns, uint32_t k_bytes, const Epilogue& epilogue, cudaStream_t stream);
+// forward NTTs of transforms [t_first, t_first + t_count) of both operands, every prime
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r,
-                        uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+                        uint32_t n, uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream);
 void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r,
                       uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+// inverse NTTs of transforms [v_first, v_first + v_count), every prime
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r,
-                        uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+                        uint32_t n, uint32_t n_sub, uint32_t v_first, uint32_t v_count, cudaStream_t stream);
+// crt_in[s*j + v][k] = residues[0][k][v*N' + j] for rho = v*N' + j in [first, first + count);
+// zero for k in [r, r')
 void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r,
-                      uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
+                      uint32_t n, uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream);
 
 struct ReduceParams {
-    const uint64_t* dots;     // [N][words]
-    uint32_t* out;            // [N][limbs]
+    const uint64_t* dots;     // [n][words]
+    uint32_t* out;            // [n][limbs]
     const uint32_t* q;        // [limbs]
     const uint32_t* minus_p;  // [limbs]  (-P) mod q
     uint32_t n, limbs, words;

@@ -16,6 +16,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <vector>
 
 #include "../../include/negacyclic.h"
 #include "gemm_tc.cuh"
@@ -55,8 +56,10 @@ namespace negacyclic::detail {
 
 constexpr uint32_t kStages = 7;  // convert, forward, pointwise, inverse, transpose, crt, reduce
 
-// conversion GEMM over the coefficients s*j + t, j in [first_j, first_j + span), all t, both operands
-void enqueue_convert(negacyclic_plan& s, uint32_t first_j, uint32_t span, cudaStream_t stream) {
+// conversion GEMM over the coefficients s*j + t, t in [t_first, t_first + t_count),
+// j in [first_j, first_j + span), both operands
+void enqueue_convert(negacyclic_plan& s, uint32_t t_first, uint32_t t_count, uint32_t first_j, uint32_t span,
+                     cudaStream_t stream) {
     const HostPlan& h = s.host;
     Epilogue convert{};
     convert.mode = kEpilogueConvert;
@@ -64,8 +67,8 @@ void enqueue_convert(negacyclic_plan& s, uint32_t first_j, uint32_t span, cudaSt
     convert.primes = s.primes;
     convert.r = s.r;
     convert.n = h.n;
-    const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span);
-    const uint32_t m = 2 * h.split * span;
+    const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span, t_first, t_count);
+    const uint32_t m = 2 * t_count * span;
     if (s.convert_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.convert_gemm, rows, m))
         launch_gemm_tensor(s.convert_gemm, convert, stream, rows, m);
     else
@@ -102,7 +105,7 @@ void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t
     launch_reduce(reduce, stream);
 }
 
-// forward NTTs, pointwise products, inverse NTTs, transpose
+// forward NTTs, pointwise products, inverse NTTs, transpose, all transforms
 void enqueue_middle(negacyclic_plan& s, cudaStream_t stream, cudaEvent_t* marks) {
     const HostPlan& h = s.host;
     const uint32_t n = h.n;
@@ -111,13 +114,13 @@ void enqueue_middle(negacyclic_plan& s, cudaStream_t stream, cudaEvent_t* marks)
         if (marks) check(cudaEventRecord(marks[stage], stream), "cudaEventRecord");
         ++stage;
     };
-    launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, n, h.n_sub, h.split, stream);
+    launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, n, h.n_sub, 0, h.split, stream);
     mark();
     launch_pointwise(s.residues, s.primes, s.zeta, s.r, n, h.n_sub, h.split, stream);
     mark();
-    launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, n, h.n_sub, h.split, stream);
+    launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, n, h.n_sub, 0, h.split, stream);
     mark();
-    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, n, h.n_sub, h.split, stream);
+    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, n, h.split, 0, n, stream);
     mark();
 }
 
@@ -125,7 +128,7 @@ void enqueue_middle(negacyclic_plan& s, cudaStream_t stream, cudaEvent_t* marks)
 // `marks` (optional, kStages events) are recorded after each stage.
 void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cudaEvent_t* marks = nullptr) {
     const HostPlan& h = s.host;
-    enqueue_convert(s, 0, h.n_sub, stream);
+    enqueue_convert(s, 0, h.split, 0, h.n_sub, stream);
     if (marks) check(cudaEventRecord(marks[0], stream), "cudaEventRecord");
     enqueue_middle(s, stream, marks ? marks + 1 : nullptr);
     enqueue_output(s, 0, h.n, d_c, stream, marks ? marks[5] : nullptr);
@@ -175,7 +178,7 @@ std::string bind_work(negacyclic_plan& s, void* arena) {
     if (!s.gemm_tensor_wanted) return "";
     std::string why_convert, why_crt;
     if (prepare_gemm_tensor(s.convert_gemm, reinterpret_cast<const uint8_t*>(s.operands), uint64_t(s.padded_limbs) * 4,
-                            RowMap::split_rows(h.n, h.n_sub, h.split, 0, h.n_sub), 2 * h.n, s.convert_weights,
+                            RowMap::split_rows(h.n, h.n_sub, h.split, 0, h.n_sub, 0, h.split), 2 * h.n, s.convert_weights,
                             4 * s.padded_r, s.k_convert, why_convert))
         s.convert_engine = NEGACYCLIC_GEMM_TENSOR;
     if (prepare_gemm_tensor(s.crt_gemm, reinterpret_cast<const uint8_t*>(s.crt_in), uint64_t(s.padded_r) * 4,
@@ -265,8 +268,9 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&s.copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&s.copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
-        // host products stream in 8 coefficient chunks once each chunk keeps 128-row GEMM tiles
-        s.chunks = (h.n_sub >= 1024 && h.n >= 8192) ? 8 : 1;
+        // host products stream in transform-ordered chunks (max(8, s) of them) once each chunk
+        // keeps 128-row GEMM tiles
+        s.chunks = (h.n_sub >= 1024 && h.n >= 8192) ? std::max(8u, h.split) : 1;
         for (uint32_t c = 0; c < s.chunks; ++c) {
             check(cudaEventCreateWithFlags(&s.in_ready[c], cudaEventDisableTiming), "cudaEventCreate");
             check(cudaEventCreateWithFlags(&s.out_ready[c], cudaEventDisableTiming), "cudaEventCreate");
@@ -447,48 +451,105 @@ void ensure_staging(negacyclic_plan& s) {
     }
 }
 
+// Streamed host products run in s.chunks chunks each way.
+// In: rows of at least 1 KB go in transform order: chunk c is transform t = c / parts, positions
+// j in [j0, j0 + span), i.e. coefficients s*j + t (one 2-D copy per operand), so the forward NTTs
+// of transform t run while later transforms are still being copied in. Narrower rows go as
+// contiguous coefficient ranges, whose forward NTTs wait for the last chunk.
+// Out: contiguous coefficient ranges; each chunk's copy-out overlaps the next chunk's CRT GEMM
+// and reduction.
+struct Chunk {
+    uint32_t t, j0, span;
+};
+
+Chunk chunk_of(const negacyclic_plan& s, uint32_t c) {
+    const uint32_t parts = s.chunks / s.host.split, span = s.host.n_sub / parts;
+    return Chunk{c / parts, (c % parts) * span, span};
+}
+
+bool transform_ordered_input(const negacyclic_plan& s) {
+    return s.chunks > 1 && s.host.split > 1 && s.host.limbs >= 256;  // chunks >= split when chunked
+}
+
+void copy_rows_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row, uint32_t rows,
+                     cudaMemcpyKind kind, cudaStream_t stream, const char* what) {
+    if (dpitch == row && spitch == row)
+        check(cudaMemcpyAsync(dst, src, row * rows, kind, stream), what);
+    else
+        check(cudaMemcpy2DAsync(dst, dpitch, src, spitch, row, rows, kind, stream), what);
+}
+
 // Enqueues a host product. Inputs: page-locked arrays go straight to the copy engine,
 // pageable ones through stage_in (the team copies chunk k+1 while chunk k is in flight).
 // Output: straight into c when c is page-locked, else into stage_out for host_finish.
 void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     const HostPlan& h = s.host;
-    const size_t row = size_t(h.limbs) * 4;
-    const uint32_t chunks = s.chunks, per = h.n / chunks, span = h.n_sub / chunks;
+    const size_t row = size_t(h.limbs) * 4, words = size_t(h.n) * h.limbs;
+    const uint32_t split = h.split, n_sub = h.n_sub, chunks = s.chunks, per = h.n / chunks;
     cudaStream_t st = s.stream;
     const bool a_locked = page_locked(a), b_locked = page_locked(b);
     s.outputs_staged = !(c && page_locked(c));
     if (!a_locked || !b_locked || s.outputs_staged) ensure_staging(s);
     check(cudaMemsetAsync(s.error_flag, 0, 4, st), "memset");
-    // rows arrive by contiguous copies (pitched copies from pageable memory run row by row),
-    // are padded and put in split-major order on the device unless they already land in place
-    // (L % 4 == 0 and s == 1), and are converted while the next chunk is in flight. The CRT
-    // word-sum buffer, written only after every chunk is converted, stages them.
-    const bool direct = s.padded_limbs == h.limbs && h.split == 1;
-    uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
-    const size_t words = size_t(h.n) * h.limbs;
-    for (uint32_t k = 0; k < chunks; ++k) {
-        const size_t first = size_t(k) * per, bytes = size_t(per) * row;
-        const uint32_t* src_a = a + first * h.limbs;
-        const uint32_t* src_b = b + first * h.limbs;
-        if (!a_locked) {
-            s.team->copy(s.stage_in + first * h.limbs, src_a, bytes);
-            src_a = s.stage_in + first * h.limbs;
+    const uint32_t* src[2] = {a, b};
+    const bool locked[2] = {a_locked, b_locked};
+    // rows land unpadded (straight in the operands when they need neither padding nor
+    // permutation) and are padded on the device; the CRT word-sum buffer, written only after
+    // every chunk is converted, stages them
+    if (transform_ordered_input(s)) {
+        const bool direct = s.padded_limbs == h.limbs;
+        uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
+        const uint32_t parts = chunks / split;
+        for (uint32_t k = 0; k < chunks; ++k) {
+            const Chunk ch = chunk_of(s, k);
+            const size_t host_row0 = size_t(split) * ch.j0 + ch.t, buf_row0 = size_t(ch.t) * n_sub + ch.j0;
+            for (int op = 0; op < 2; ++op) {
+                const uint32_t* from = src[op] + host_row0 * h.limbs;
+                size_t pitch = split * row;
+                if (!locked[op]) {  // gather the chunk's rows into stage_in at their split-major places
+                    uint32_t* gathered = s.stage_in + (op * size_t(h.n) + buf_row0) * h.limbs;
+                    s.team->copy_rows(gathered, row, from, pitch, row, ch.span);
+                    from = gathered;
+                    pitch = row;
+                }
+                copy_rows_async(staged + (op * size_t(h.n) + buf_row0) * h.limbs, row, from, pitch, row, ch.span,
+                                cudaMemcpyHostToDevice, s.copy_in, "copy in");
+            }
+            check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
+            check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
+            if (!direct)
+                launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, 1, uint32_t(buf_row0), ch.span, st);
+            enqueue_convert(s, ch.t, 1, ch.j0, ch.span, st);
+            if (k % parts == parts - 1)  // transform t complete: its forward NTTs, both operands
+                launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, ch.t, 1, st);
         }
-        if (!b_locked) {
-            s.team->copy(s.stage_in + words + first * h.limbs, src_b, bytes);
-            src_b = s.stage_in + words + first * h.limbs;
+    } else {
+        const bool direct = s.padded_limbs == h.limbs && split == 1;
+        uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
+        for (uint32_t k = 0; k < chunks; ++k) {
+            const size_t first = size_t(k) * per, bytes = size_t(per) * row;
+            for (int op = 0; op < 2; ++op) {
+                const uint32_t* from = src[op] + first * h.limbs;
+                if (!locked[op]) {
+                    s.team->copy(s.stage_in + op * words + first * h.limbs, from, bytes);
+                    from = s.stage_in + op * words + first * h.limbs;
+                }
+                check(cudaMemcpyAsync(staged + op * words + first * h.limbs, from, bytes, cudaMemcpyHostToDevice,
+                                      s.copy_in),
+                      "copy in");
+            }
+            check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
+            check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
+            if (!direct)
+                launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, split, uint32_t(first), per, st);
+            const uint32_t span = n_sub / chunks;  // coefficients [first, first + per): j in [k span, (k+1) span)
+            enqueue_convert(s, 0, split, k * span, span, st);
         }
-        check(cudaMemcpyAsync(staged + first * h.limbs, src_a, bytes, cudaMemcpyHostToDevice, s.copy_in), "copy a");
-        check(cudaMemcpyAsync(staged + (size_t(h.n) + first) * h.limbs, src_b, bytes, cudaMemcpyHostToDevice,
-                              s.copy_in),
-              "copy b");
-        check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
-        check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
-        if (!direct)
-            launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, h.split, uint32_t(first), per, st);
-        enqueue_convert(s, k * span, span, st);
+        launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, 0, split, st);
     }
-    enqueue_middle(s, st, nullptr);
+    launch_pointwise(s.residues, s.primes, s.zeta, s.r, h.n, n_sub, split, st);
+    launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, h.n, n_sub, 0, split, st);
+    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, 0, h.n, st);
     // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
     uint32_t* dst = s.outputs_staged ? s.stage_out : c;
     for (uint32_t k = 0; k <= chunks; ++k) {
