@@ -414,7 +414,8 @@ def run_batch(args):
 
 
 def run_serve(args):
-    """Poisson arrivals over 8 sessions (fixed L and q each, N per request); p50/p99 and products/s."""
+    """Poisson arrivals over 8 sessions (fixed L and q each, N per request) at each offered rate;
+    p50/p99 latency and products/s, then the same request mix through the plain per-call path."""
     import torch
 
     torch.cuda.set_device(0)
@@ -437,46 +438,73 @@ def run_serve(args):
                 b = torch.from_numpy(inputs.random_operand(rng, n, q).view(np.int32)).pin_memory()
                 pairs.append((a.numpy().view(np.uint32), b.numpy().view(np.uint32)))
             pool[n] = pairs
-        sessions.append((sid, limbs, pool))
+        sessions.append((sid, limbs, q, pool))
     outputs = {}
-    for sid, limbs, pool in sessions:
+    for sid, limbs, _, pool in sessions:
         for n in SIZES:
             outputs[(sid, n)] = [torch.empty((n, limbs), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
                                  for _ in range(args.slots + 1)]
     log("sessions and buffers ready")
-    # Poisson arrival schedule
-    t = 0.0
-    schedule = []
-    while t < args.duration:
-        t += rng.exponential(1.0 / args.rate)
-        s_index = int(rng.integers(len(sessions)))
-        schedule.append((t, s_index, int(rng.choice(SIZES)), int(rng.integers(args.serve_pairs))))
-    ids = []
-    out_counter = {}
-    start = time.perf_counter()
-    for when, s_index, n, k in schedule:
-        delay = when - (time.perf_counter() - start)
-        if delay > 0:
-            time.sleep(delay)
-        sid, limbs, pool = sessions[s_index]
-        ring = outputs[(sid, n)]
-        slot = out_counter.get((sid, n), 0)
-        out_counter[(sid, n)] = slot + 1
-        a, b = pool[n][k]
-        ids.append(server.submit(sid, a, b, out=ring[slot % len(ring)]))
-    log(f"submitted {len(ids)} requests")
-    latencies = [server.wait(rid)[1] for rid in ids]
-    elapsed = time.perf_counter() - start
-    log(f"all done in {elapsed:.1f} s, pipeline status {fpc.pipeline_status()}")
+
+    def schedule_for(rate, duration):
+        t, out = 0.0, []
+        while t < duration:
+            t += rng.exponential(1.0 / rate)
+            out.append((t, int(rng.integers(len(sessions))), int(rng.choice(SIZES)), int(rng.integers(args.serve_pairs))))
+        return out
+
+    runs = []
+    for rate in [float(x) for x in args.rates.split(",")]:
+        # offered load above capacity queues up: a shorter arrival window keeps the drain bounded
+        duration = args.duration if rate <= 400 else args.duration * 400 / rate
+        schedule = schedule_for(rate, duration)
+        ids, out_counter = [], {}
+        start = time.perf_counter()
+        for when, s_index, n, k in schedule:
+            delay = when - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            sid, limbs, _, pool = sessions[s_index]
+            ring = outputs[(sid, n)]
+            slot = out_counter.get((sid, n), 0)
+            out_counter[(sid, n)] = slot + 1
+            a, b = pool[n][k]
+            ids.append(server.submit(sid, a, b, out=ring[slot % len(ring)]))
+        latencies = np.array([server.wait(rid)[1] for rid in ids])
+        elapsed = time.perf_counter() - start
+        runs.append({"offered_rate": rate, "arrival_window_s": round(duration, 3), "requests": len(ids),
+                     "products_per_s": len(ids) / elapsed, "p50_ms": float(np.percentile(latencies, 50)),
+                     "p99_ms": float(np.percentile(latencies, 99)), "mean_ms": float(latencies.mean()),
+                     "elapsed_s": round(elapsed, 3)})
+        log(f"rate {rate:g}: {runs[-1]}")
     stats = server.stats()
     server.close()
-    lat = np.array(latencies)
-    line = {"metric": f"served products/s at {args.rate:g} req/s Poisson, 8 sessions, N in 4096..65536",
-            "value": len(ids) / elapsed, "unit": "products/s", "mode": "serving (continuous batching)",
-            "requests": len(ids), "offered_rate": args.rate, "duration_s": elapsed,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "slots": args.slots, "hbm_budget_gb": args.budget_gb,
-            "session_max_limbs": max_limbs, "failed": stats["failed"], "data": "synthetic (seed 200)"}
+
+    # the same request mix through the plain per-call path (negacyclic_run, page-locked buffers),
+    # one (session, N) plan at a time
+    mix = schedule_for(1.0, float(args.plain_requests))[: args.plain_requests]
+    groups = {}
+    for _, s_index, n, k in mix:
+        groups.setdefault((s_index, n), []).append(k)
+    plain_s = 0.0
+    for (s_index, n), ks in groups.items():
+        sid, limbs, q, pool = sessions[s_index]
+        plan = fpc.Plan(n, 32 * limbs, limbs, q)
+        out = outputs[(sid, n)][0]
+        plan.run(*pool[n][ks[0]], out=out)  # warm-up
+        for k in ks:
+            t0 = time.perf_counter()
+            plan.run(*pool[n][k], out=out)
+            plain_s += time.perf_counter() - t0
+        plan.close()
+    plain_value = len(mix) / plain_s
+    best = max(r["products_per_s"] for r in runs)
+    line = {"metric": "served products/s, Poisson arrivals, 8 sessions (fixed q, L each), N in 4096..65536",
+            "value": best, "unit": "products/s", "mode": "serving (continuous batching)", "runs": runs,
+            "plain_per_call_products_per_s": plain_value, "plain_requests": len(mix),
+            "served_over_plain": best / plain_value, "slots": args.slots, "hbm_budget_gb": args.budget_gb,
+            "session_limbs": [limbs for _, limbs, _, _ in sessions], "failed": stats["failed"],
+            "data": "synthetic (seed 200)"}
     print(json.dumps(line), flush=True)
 
 
@@ -497,8 +525,10 @@ def main():
     parser.add_argument("--lanes", type=int, default=0, help="batch: concurrent streams (0 = 4)")
     parser.add_argument("--tune", action="store_true", help="batch: run the autotuner for uncached shapes")
     parser.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
-    parser.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
-    parser.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    parser.add_argument("--rates", default="200,1000,5000", help="serve: Poisson arrival rates (requests/s)")
+    parser.add_argument("--duration", type=float, default=10.0,
+                        help="serve: seconds of arrivals (scaled down above 400 requests/s)")
+    parser.add_argument("--plain-requests", type=int, default=200, help="serve: requests of the plain comparison")
     parser.add_argument("--slots", type=int, default=4, help="serve: concurrent requests")
     parser.add_argument("--budget-gb", type=float, default=60.0, help="serve: HBM budget (GiB)")
     parser.add_argument("--serve-max-limbs", type=int, default=1747, help="serve: largest session L")

@@ -4,12 +4,20 @@
 // src/main.cpp:164-204). A session fixes (W, L, q); its plans (one per ring
 // size N, parameter tables resident on the device) are built when the session
 // opens or on the first request of a new N. Requests are submitted from any
-// thread and return at once. One dispatcher thread admits queued requests, in
-// arrival order, whenever a stream slot is free and the request's device memory
-// (work space + operand/result buffers, from a stream-ordered pool) fits the
-// HBM budget; each admitted request runs copy-in, product and copy-out on its
-// slot's stream, so requests that arrive while others run overlap with them on
-// the device. Completion is signalled by a host callback on the slot's stream.
+// thread and return at once.
+//
+// Requests flow through a three-stream pipeline:
+//   copy-in   operands of request i+1 (host -> device, own buffers from a stream-ordered pool)
+//   compute   request i: pad, product (one work arena shared by every request, since the
+//             compute stream runs them one after another)
+//   copy-out  result of request i-1 (device -> host), then the buffers are freed and a host
+//             callback completes the request.
+// One dispatcher thread admits queued requests in arrival order while fewer than `slots` are in
+// the pipeline and the request's operand buffers (plus any growth of the shared arena) fit the
+// HBM budget next to the resident plan tables. A request that arrives while others are on the
+// GPU joins the pipeline as soon as a place and memory free up, so its copies overlap their
+// compute. With one compute stream the CTA-pair GEMM kernel is used; concurrent launches of
+// that kernel from several streams stalled, so a process runs one server per device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,13 +49,6 @@ struct Session {
     std::map<uint32_t, std::unique_ptr<negacyclic_plan>> plans;  // by N
 };
 
-struct Request;
-
-struct Slot {
-    cudaStream_t stream = nullptr;
-    Request* busy = nullptr;
-};
-
 struct Request {
     uint64_t id = 0;
     uint32_t session = 0, n = 0;
@@ -58,8 +59,8 @@ struct Request {
     int status = NEGACYCLIC_OK;
     std::string error;
     bool done = false;
-    size_t bytes = 0;  // device memory held while in flight
-    uint32_t slot = 0;
+    size_t bytes = 0;  // operand/result buffers held while in flight
+    cudaEvent_t copied_in = nullptr, computed = nullptr;
     struct negacyclic_server* server = nullptr;
 };
 
@@ -68,11 +69,16 @@ struct Request {
 struct negacyclic_server {
     int device = 0;
     uint64_t budget = 0, resident = 0, in_flight = 0;
+    uint32_t slots = 0, active = 0;  // pipeline depth, requests in it
     std::vector<Session> sessions;
-    std::vector<Slot> slots;
     std::deque<Request*> pending;
     std::map<uint64_t, std::unique_ptr<Request>> requests;
     uint64_t next_id = 1;
+    cudaStream_t copy_in = nullptr, compute = nullptr, copy_out = nullptr;
+    void* arena = nullptr;  // shared work space, stream-ordered on `compute`
+    size_t arena_bytes = 0;
+    std::vector<cudaEvent_t> spare_events;  // completed events, reusable
+    std::vector<cudaEvent_t> all_events;
     std::mutex mu;
     std::condition_variable wake, finished;
     std::thread dispatcher;
@@ -83,30 +89,26 @@ struct negacyclic_server {
 
     void run();
     bool admit_one(std::unique_lock<std::mutex>& lock);
+    cudaEvent_t take_event();
+    void fail_head(Request* r, int status, const std::string& error);
     static void CUDART_CB on_done(void* data);
 };
 
 namespace {
 
-size_t request_bytes(const negacyclic_plan& plan) {
-    const size_t io = (size_t(plan.host.n) * plan.host.limbs * 4 + 255) / 256 * 256;
-    return plan.work_bytes + 3 * io;
+size_t io_bytes(const negacyclic_plan& plan) {
+    return 3 * ((size_t(plan.host.n) * plan.host.limbs * 4 + 255) / 256 * 256);
 }
 
 // Builds a session plan for ring size n. Must be called WITHOUT the server lock:
 // plan creation can synchronise the device, and the completion callbacks of
 // requests in flight need the lock to finish.
-int build_session_plan(int device, uint32_t slots, uint32_t w, uint32_t limbs, const uint32_t* q, uint32_t n,
+int build_session_plan(int device, uint32_t w, uint32_t limbs, const uint32_t* q, uint32_t n,
                        negacyclic_plan** out) {
     negacyclic_options o{};
     o.device = device;
     o.external_work = 1;
-    const int status = negacyclic_init(n, w, limbs, q, &o, out);
-    if (status != NEGACYCLIC_OK) return status;
-    // requests on several slots run concurrently: they use the single-CTA tensor-core
-    // kernel, because concurrent launches of the CTA-pair kernel from several streams stalled
-    if (slots > 1) (*out)->gemm_pairs_allowed = false;
-    return NEGACYCLIC_OK;
+    return negacyclic_init(n, w, limbs, q, &o, out);
 }
 
 // Adds a built plan to a session under the budget. Caller holds the lock.
@@ -129,6 +131,30 @@ int install_plan(negacyclic_server& s, Session& session, uint32_t n, negacyclic_
 
 }  // namespace
 
+// Caller holds the lock.
+cudaEvent_t negacyclic_server::take_event() {
+    if (!spare_events.empty()) {
+        cudaEvent_t e = spare_events.back();
+        spare_events.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    all_events.push_back(e);
+    return e;
+}
+
+// Completes the queue head `r` (already popped) with an error. Caller holds the lock.
+void negacyclic_server::fail_head(Request* r, int status, const std::string& error) {
+    r->status = status;
+    r->error = error;
+    r->done = true;
+    r->finished = now_ms();
+    ++failed;
+    finished.notify_all();
+}
+
+// Runs on the copy-out stream after the result landed: no CUDA calls allowed here.
 void CUDART_CB negacyclic_server::on_done(void* data) {
     Request* r = static_cast<Request*>(data);
     negacyclic_server* s = r->server;
@@ -136,7 +162,9 @@ void CUDART_CB negacyclic_server::on_done(void* data) {
     r->finished = now_ms();
     r->done = true;
     s->in_flight -= r->bytes;
-    s->slots[r->slot].busy = nullptr;
+    --s->active;
+    s->spare_events.push_back(r->copied_in);  // both completed before this callback
+    s->spare_events.push_back(r->computed);
     ++s->completed;
     s->latencies.push_back(r->finished - r->submitted);
     s->last_finish = std::max(s->last_finish, r->finished);
@@ -144,14 +172,11 @@ void CUDART_CB negacyclic_server::on_done(void* data) {
     s->wake.notify_one();
 }
 
-// Admits the head of the queue if a slot is free and its memory fits the budget.
+// Admits the head of the queue if the pipeline has room and its memory fits the budget.
 bool negacyclic_server::admit_one(std::unique_lock<std::mutex>& lock) {
-    if (pending.empty()) return false;
-    auto free_slot = std::find_if(slots.begin(), slots.end(), [](const Slot& x) { return x.busy == nullptr; });
-    if (free_slot == slots.end()) return false;
+    if (pending.empty() || active >= slots) return false;
     Request* r = pending.front();
     negacyclic_plan* plan = nullptr;
-    int status = NEGACYCLIC_OK;
     {
         Session& session = sessions[r->session];
         auto it = session.plans.find(r->n);
@@ -163,7 +188,7 @@ bool negacyclic_server::admit_one(std::unique_lock<std::mutex>& lock) {
             const uint32_t n = r->n, session_id = r->session;
             lock.unlock();
             negacyclic_plan* built = nullptr;
-            status = build_session_plan(device, uint32_t(slots.size()), w, limbs, q.data(), n, &built);
+            int status = build_session_plan(device, w, limbs, q.data(), n, &built);
             std::string error = status == NEGACYCLIC_OK ? "" : negacyclic_last_error();
             lock.lock();
             if (status == NEGACYCLIC_OK) status = install_plan(*this, sessions[session_id], n, built, &plan);
@@ -171,75 +196,70 @@ bool negacyclic_server::admit_one(std::unique_lock<std::mutex>& lock) {
             if (status != NEGACYCLIC_OK) {
                 r = pending.front();  // the queue head is unchanged: only this thread pops it
                 pending.pop_front();
-                r->status = status;
-                r->error = error;
-                r->done = true;
-                r->finished = now_ms();
-                ++failed;
-                finished.notify_all();
-                return true;
+                fail_head(r, status, error);
             }
-            return true;  // re-evaluate slots and budget with the plan in place
+            return true;  // re-evaluate room and budget with the plan in place
         }
     }
-    auto reject = [&](int code, const std::string& why) {
-        pending.pop_front();
-        r->status = code;
-        r->error = why;
-        r->done = true;
-        r->finished = now_ms();
-        ++failed;
-        finished.notify_all();
-        return true;
-    };
-    const size_t need = request_bytes(*plan);
-    if (resident + in_flight + need > budget) {
-        const bool idle = std::all_of(slots.begin(), slots.end(), [](const Slot& x) { return x.busy == nullptr; });
-        if (idle) return reject(NEGACYCLIC_ENOMEM, "request exceeds the HBM budget");
+    const size_t need = io_bytes(*plan);
+    const size_t arena_need = std::max(arena_bytes, plan->work_bytes);
+    if (resident + arena_need + in_flight + need > budget) {
+        if (active == 0) {  // nothing in flight will free memory: it can never fit
+            pending.pop_front();
+            fail_head(r, NEGACYCLIC_ENOMEM, "request exceeds the HBM budget");
+            return true;
+        }
         return false;  // wait for memory to free up (arrival order is kept)
     }
     pending.pop_front();
-    const uint32_t index = uint32_t(free_slot - slots.begin());
-    free_slot->busy = r;
-    r->slot = index;
     r->bytes = need;
     r->admitted = now_ms();
     in_flight += need;
-    cudaStream_t st = free_slot->stream;
-    // enqueue without holding the lock (copies from pageable memory block the host)
-    lock.unlock();
+    ++active;
     std::string error;
+    bool locked = true;
     try {
-        void* mem = nullptr;
-        check(cudaMallocAsync(&mem, need, st), "cudaMallocAsync");
-        const std::string why = bind_work(*plan, mem);
+        r->copied_in = take_event();
+        r->computed = take_event();
+        if (arena_need > arena_bytes) {  // grow the shared arena in compute-stream order
+            void* grown = nullptr;
+            check(cudaMallocAsync(&grown, arena_need, compute), "cudaMallocAsync");
+            if (arena) check(cudaFreeAsync(arena, compute), "cudaFreeAsync");
+            arena = grown;
+            arena_bytes = arena_need;
+        }
+        void* work = arena;
+        // enqueue without holding the lock (copies from pageable memory block the host)
+        lock.unlock();
+        locked = false;
+        uint8_t* io = nullptr;
+        check(cudaMallocAsync(reinterpret_cast<void**>(&io), need, copy_in), "cudaMallocAsync");
+        const size_t words = size_t(r->n) * plan->host.limbs, slot = need / 3;
+        uint32_t* d_a = reinterpret_cast<uint32_t*>(io);
+        uint32_t* d_b = reinterpret_cast<uint32_t*>(io + slot);
+        uint32_t* d_c = reinterpret_cast<uint32_t*>(io + 2 * slot);
+        check(cudaMemcpyAsync(d_a, r->a, words * 4, cudaMemcpyHostToDevice, copy_in), "copy a");
+        check(cudaMemcpyAsync(d_b, r->b, words * 4, cudaMemcpyHostToDevice, copy_in), "copy b");
+        check(cudaEventRecord(r->copied_in, copy_in), "cudaEventRecord");
+        check(cudaStreamWaitEvent(compute, r->copied_in, 0), "cudaStreamWaitEvent");
+        // only this thread binds plans; kernel arguments are copied at launch
+        const std::string why = bind_work(*plan, work);
         if (!why.empty()) throw CudaError{cudaErrorInvalidValue, "bind_work"};
-        const size_t words = size_t(r->n) * plan->host.limbs;
-        const size_t io = (words * 4 + 255) / 256 * 256;
-        uint8_t* base = static_cast<uint8_t*>(mem) + plan->work_bytes;
-        uint32_t* d_a = reinterpret_cast<uint32_t*>(base);
-        uint32_t* d_b = reinterpret_cast<uint32_t*>(base + io);
-        uint32_t* d_c = reinterpret_cast<uint32_t*>(base + 2 * io);
-        check(cudaMemcpyAsync(d_a, r->a, words * 4, cudaMemcpyHostToDevice, st), "copy a");
-        check(cudaMemcpyAsync(d_b, r->b, words * 4, cudaMemcpyHostToDevice, st), "copy b");
-        enqueue_device_product(*plan, d_a, d_b, d_c, st);
-        check(cudaMemcpyAsync(r->c, d_c, words * 4, cudaMemcpyDeviceToHost, st), "copy c");
-        check(cudaFreeAsync(mem, st), "cudaFreeAsync");
-        check(cudaLaunchHostFunc(st, &negacyclic_server::on_done, r), "cudaLaunchHostFunc");
+        enqueue_device_product(*plan, d_a, d_b, d_c, compute);
+        check(cudaEventRecord(r->computed, compute), "cudaEventRecord");
+        check(cudaStreamWaitEvent(copy_out, r->computed, 0), "cudaStreamWaitEvent");
+        check(cudaMemcpyAsync(r->c, d_c, words * 4, cudaMemcpyDeviceToHost, copy_out), "copy c");
+        check(cudaFreeAsync(io, copy_out), "cudaFreeAsync");
+        check(cudaLaunchHostFunc(copy_out, &negacyclic_server::on_done, r), "cudaLaunchHostFunc");
     } catch (const CudaError& e) {
         error = std::string(e.where) + ": " + cudaGetErrorString(e.code);
         cudaGetLastError();
     }
-    lock.lock();
+    if (!locked) lock.lock();
     if (!error.empty()) {  // nothing was left on the stream that calls back
-        r->status = NEGACYCLIC_ECUDA;
-        r->error = error;
-        r->done = true;
-        r->finished = now_ms();
         in_flight -= need;
-        free_slot->busy = nullptr;
-        ++failed;
-        finished.notify_all();
+        --active;
+        fail_head(r, NEGACYCLIC_ECUDA, error);
     }
     return true;
 }
@@ -267,17 +287,19 @@ int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_s
     auto s = std::make_unique<negacyclic_server>();
     s->device = device;
     s->budget = o.hbm_budget ? o.hbm_budget : (uint64_t(60) << 30);
+    s->slots = o.slots ? o.slots : 4;
     DeviceGuard guard(device);
     try {
-        s->slots.resize(o.slots ? o.slots : 4);
-        for (Slot& slot : s->slots)
-            check(cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (cudaStream_t* st : {&s->copy_in, &s->compute, &s->copy_out})
+            check(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate");
         // keep freed request memory in the pool up to the budget instead of returning it
         cudaMemPool_t pool = nullptr;
         check(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
         uint64_t threshold = s->budget;
         check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
     } catch (const CudaError& e) {
+        for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
+            if (st) cudaStreamDestroy(st);
         return cuda_failure(e);
     }
     negacyclic_server* raw = s.release();
@@ -303,7 +325,7 @@ int negacyclic_server_open_session(negacyclic_server* s, uint32_t w, uint32_t li
     }
     for (uint32_t i = 0; ns && i < count; ++i) {  // resident plans for the announced ring sizes
         negacyclic_plan* plan = nullptr;
-        int status = build_session_plan(s->device, uint32_t(s->slots.size()), w, limbs, q, ns[i], &plan);
+        int status = build_session_plan(s->device, w, limbs, q, ns[i], &plan);
         if (status != NEGACYCLIC_OK) return status;
         std::lock_guard<std::mutex> lock(s->mu);
         negacyclic_plan* installed = nullptr;
@@ -362,7 +384,7 @@ int negacyclic_server_get_stats(negacyclic_server* s, negacyclic_server_stats* o
     out->completed = s->completed;
     out->failed = s->failed;
     out->queued = s->pending.size();
-    out->resident_bytes = s->resident;
+    out->resident_bytes = s->resident + s->arena_bytes;
     out->in_flight_bytes = s->in_flight;
     std::vector<double> lat = s->latencies;
     if (!lat.empty()) {
@@ -391,11 +413,12 @@ void negacyclic_server_free(negacyclic_server* s) {
         int previous = 0;
         cudaGetDevice(&previous);
         cudaSetDevice(s->device);
-        for (Slot& slot : s->slots)
-            if (slot.stream) {
-                cudaStreamSynchronize(slot.stream);
-                cudaStreamDestroy(slot.stream);
-            }
+        for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
+            if (st) cudaStreamSynchronize(st);
+        if (s->arena) cudaFree(s->arena);
+        for (cudaEvent_t e : s->all_events) cudaEventDestroy(e);
+        for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
+            if (st) cudaStreamDestroy(st);
         cudaSetDevice(previous);
     }
     delete s;
