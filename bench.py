@@ -383,7 +383,7 @@ def run_batch(args):
         stop.synchronize()
         plain_ms += start.elapsed_time(stop) / max(1, args.steps // 2)
     log(f"plain {plain_ms:.1f} ms per batch, pipeline status {fpc.pipeline_status()}")
-    # host arrays (page-locked): batched (lanes overlap copies with other products) vs one call each
+    # host arrays (page-locked): batched (copy-in, compute and copy-out streams overlap) vs one call each
     pinned = lambda x: torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)  # noqa: E731
     ha = [pinned(a) for _, _, _, a, _ in instances]
     hb = [pinned(b) for _, _, _, _, b in instances]
@@ -407,7 +407,7 @@ def run_batch(args):
                          "plain_products_per_s": len(instances) / (host_plain_ms / 1000),
                          "batched_over_plain": host_plain_ms / host_batched_ms,
                          "bytes_per_batch": int(sum(3 * a.nbytes for _, _, _, a, _ in instances))},
-            "lanes": args.lanes or min(len(instances), 4), "tuned": bool(args.tune), "setup_s": setup_s,
+            "lanes": args.lanes or 1, "tuned": bool(args.tune), "setup_s": setup_s,
             "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seed 100)"}
     print(json.dumps(line), flush=True)
     batch.close()
@@ -522,7 +522,7 @@ def main():
     parser.add_argument("--mode", choices=("plain", "batch", "serve"), default="plain",
                         help="plain: the benchmark line; batch / serve: the batched and serving forms")
     parser.add_argument("--count", type=int, default=64, help="batch: number of uneven products")
-    parser.add_argument("--lanes", type=int, default=0, help="batch: concurrent streams (0 = 4)")
+    parser.add_argument("--lanes", type=int, default=0, help="batch: compute lanes (0 = 1)")
     parser.add_argument("--tune", action="store_true", help="batch: run the autotuner for uncached shapes")
     parser.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     parser.add_argument("--rates", default="200,1000,5000", help="serve: Poisson arrival rates (requests/s)")

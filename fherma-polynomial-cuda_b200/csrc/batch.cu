@@ -8,11 +8,15 @@
 //     length N' = N/s and the prime set) and the GEMM kernel (CTA-pair 256x256
 //     tiles, single-CTA 128x256 tiles, or the SIMT kernel) by timing each
 //     candidate on the device; results are cached in a text file;
-//   * instances are assigned longest-first to `lanes` streams; each lane owns
-//     one work arena (sized for its largest instance) that its instances use
-//     one after another;
+//   * instances are assigned longest-first to `lanes` compute streams (one by
+//     default: a large product fills the GPU by itself, and a single lane may use
+//     the CTA-pair GEMM kernel); each lane owns one work arena (sized for its
+//     largest instance) that its instances use one after another;
 //   * the whole batch — every lane's chain of products — is captured once into a
-//     CUDA graph, so a batch run is a single cudaGraphLaunch.
+//     CUDA graph, so a batch run is a single cudaGraphLaunch;
+//   * with host arrays, operand copies run on a copy-in stream and result copies
+//     on a copy-out stream, so instance i's compute overlaps the copy-in of the
+//     instances after it and the copy-out of those before it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -150,7 +154,8 @@ struct negacyclic_batch {
     std::vector<void*> arenas;
     void* io = nullptr;
     std::vector<size_t> io_offset;  // a, then b, then c per instance
-    cudaStream_t capture = nullptr;
+    cudaStream_t capture = nullptr, copy_in = nullptr, copy_out = nullptr;
+    std::vector<cudaEvent_t> copied_in, computed;  // per instance, host-array runs
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> joins;
     cudaGraph_t graph = nullptr;
@@ -164,6 +169,10 @@ struct negacyclic_batch {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         for (cudaEvent_t e : joins) cudaEventDestroy(e);
+        for (cudaEvent_t e : copied_in) cudaEventDestroy(e);
+        for (cudaEvent_t e : computed) cudaEventDestroy(e);
+        if (copy_in) cudaStreamDestroy(copy_in);
+        if (copy_out) cudaStreamDestroy(copy_out);
         if (fork) cudaEventDestroy(fork);
         for (cudaStream_t s : lanes) cudaStreamDestroy(s);
         if (capture) cudaStreamDestroy(capture);
@@ -235,7 +244,7 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
         }
 
         // 2. longest-first assignment to lanes
-        const uint32_t lanes = o.lanes ? std::min(o.lanes, count) : std::min<uint32_t>(count, 4);
+        const uint32_t lanes = o.lanes ? std::min(o.lanes, count) : 1u;
         // Products on several lanes run concurrently: they use the single-CTA tensor-core kernel,
         // because concurrent launches of the CTA-pair (cluster) kernel from several streams stalled.
         if (lanes > 1)
@@ -278,6 +287,14 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
             }
         check(cudaMalloc(&b->io, io_bytes), "cudaMalloc");
         check(cudaMemset(b->io, 0, io_bytes), "cudaMemset");
+        check(cudaStreamCreateWithFlags(&b->copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&b->copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
+        b->copied_in.resize(count);
+        b->computed.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            check(cudaEventCreateWithFlags(&b->copied_in[i], cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&b->computed[i], cudaEventDisableTiming), "cudaEventCreate");
+        }
 
         // 4. capture every lane's chain of products into one graph
         check(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -355,23 +372,26 @@ int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const ui
     if (!b || !a || !bb || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
     DeviceGuard guard(b->device);
     try {
-        // per lane: copy in, product, copy out, instance after instance; lanes overlap each other
-        const uint32_t count = uint32_t(b->plans.size());
-        size_t issued = 0;
+        // issue order: round-robin over the lanes' sequences, so every lane gets work early
+        std::vector<uint32_t> order;
         std::vector<size_t> next(b->lanes.size(), 0);
-        while (issued < count) {  // round-robin issue so pageable copies of one lane overlap the others' compute
-            for (uint32_t lane = 0; lane < b->lanes.size(); ++lane) {
-                if (next[lane] >= b->lane_order[lane].size()) continue;
-                const uint32_t i = b->lane_order[lane][next[lane]++];
-                const size_t bytes = b->words(i) * 4;
-                cudaStream_t st = b->lanes[lane];
-                check(cudaMemcpyAsync(b->slot(i, 0), a[i], bytes, cudaMemcpyHostToDevice, st), "copy a");
-                check(cudaMemcpyAsync(b->slot(i, 1), bb[i], bytes, cudaMemcpyHostToDevice, st), "copy b");
-                enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), st);
-                check(cudaMemcpyAsync(c[i], b->slot(i, 2), bytes, cudaMemcpyDeviceToHost, st), "copy c");
-                ++issued;
-            }
+        while (order.size() < b->plans.size())
+            for (uint32_t lane = 0; lane < b->lanes.size(); ++lane)
+                if (next[lane] < b->lane_order[lane].size()) order.push_back(b->lane_order[lane][next[lane]++]);
+        // copy-in -> compute (the instance's lane) -> copy-out, linked by events
+        for (uint32_t i : order) {
+            const size_t bytes = b->words(i) * 4;
+            check(cudaMemcpyAsync(b->slot(i, 0), a[i], bytes, cudaMemcpyHostToDevice, b->copy_in), "copy a");
+            check(cudaMemcpyAsync(b->slot(i, 1), bb[i], bytes, cudaMemcpyHostToDevice, b->copy_in), "copy b");
+            check(cudaEventRecord(b->copied_in[i], b->copy_in), "cudaEventRecord");
+            cudaStream_t lane = b->lanes[b->lane_of[i]];
+            check(cudaStreamWaitEvent(lane, b->copied_in[i], 0), "cudaStreamWaitEvent");
+            enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), lane);
+            check(cudaEventRecord(b->computed[i], lane), "cudaEventRecord");
+            check(cudaStreamWaitEvent(b->copy_out, b->computed[i], 0), "cudaStreamWaitEvent");
+            check(cudaMemcpyAsync(c[i], b->slot(i, 2), bytes, cudaMemcpyDeviceToHost, b->copy_out), "copy c");
         }
+        check(cudaStreamSynchronize(b->copy_out), "batch");
         for (cudaStream_t st : b->lanes) check(cudaStreamSynchronize(st), "batch");
     } catch (const CudaError& e) {
         return cuda_failure(e);

@@ -91,9 +91,10 @@ int negacyclic_get_info(const negacyclic_plan* plan, negacyclic_info* info);
 /*
  * Host-to-host product: a, b, c are host arrays of n*limbs words (c may alias
  * neither input). Copies in, computes, copies out; returns when c is written.
- * Streamed in coefficient chunks: copies of chunk k+1 overlap the conversion of
- * chunk k on the way in, and the CRT/reduction of chunk k+1 overlaps the copy-out
- * of chunk k on the way out. Page-locked host memory (cudaHostAlloc /
+ * Streamed in chunks: copies of chunk k+1 overlap the conversion of chunk k on
+ * the way in (rows of 1 KB or more go transform by transform, so each transform's
+ * forward NTTs also overlap later copies), and the CRT/reduction of chunk k+1
+ * overlaps the copy-out of chunk k on the way out. Page-locked host memory (cudaHostAlloc /
  * cudaHostRegister) is read and written by DMA directly; pageable memory goes
  * through the plan's page-locked staging buffers, filled and drained by a team of
  * host threads.
@@ -210,8 +211,8 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
  * New in this library (the reference runs one product per harness call,
  * src/main.cpp:164-204). Instances are planned individually (an autotuner picks
  * each shape's ring split and GEMM kernel by timing them, cached in a text file),
- * assigned longest-first to concurrent lanes that share one work arena each,
- * and captured into a single CUDA graph.
+ * assigned longest-first to compute lanes (one by default) that share one work
+ * arena each, and captured into a single CUDA graph.
  */
 typedef struct negacyclic_batch negacyclic_batch;
 
@@ -221,7 +222,7 @@ typedef struct {
 } negacyclic_point;
 
 typedef struct {
-    uint32_t lanes;          /* concurrent streams; 0 = min(count, 4) */
+    uint32_t lanes;          /* concurrent compute streams; 0 = 1 (lanes > 1 use single-CTA GEMM tiles) */
     uint32_t tune;           /* 1: time candidate configurations for shapes not in the cache */
     int32_t device;          /* -1 = current device */
     uint32_t reserved0;
@@ -253,7 +254,8 @@ int negacyclic_batch_run_device(negacyclic_batch* batch, void* stream);
  * Must not overlap other runs of the same batch (instances share lane work spaces). */
 int negacyclic_batch_run_one(negacyclic_batch* batch, uint32_t index, void* stream);
 
-/* Host arrays a[i], b[i], c[i] per instance; copies overlap other lanes' products. Blocking. */
+/* Host arrays a[i], b[i], c[i] per instance: copy-in, compute and copy-out streams overlap
+ * (instance i computes while later operands copy in and earlier results copy out). Blocking. */
 int negacyclic_batch_run(negacyclic_batch* batch, const uint32_t* const* a, const uint32_t* const* b,
                          uint32_t* const* c);
 

@@ -58,6 +58,17 @@ def test_batch_graph_matches_oracle_and_plain_path(fpc, inputs, oracle, cudart):
         assert lanes == {0, 1, 2}
 
 
+def test_batch_default_single_lane_pipeline(fpc, inputs, oracle):
+    """One compute lane (CTA-pair GEMMs) with copy-in / copy-out streams, host arrays in and out."""
+    points = uneven_points(inputs, 8, 13, sizes=(1024, 4096, 8192), limb_range=(16, 300))
+    with fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in points]) as batch:
+        assert {batch.info(i)["lane"] for i in range(len(points))} == {0}
+        for _ in range(2):
+            results = batch.run([p[3] for p in points], [p[4] for p in points])
+            for (n, l, q, a, b), c in zip(points, results):
+                assert np.array_equal(c, oracle.kronecker(q, a, b)), (n, l)
+
+
 def test_batch_host_path_and_autotuner(fpc, inputs, oracle, tmp_path):
     points = uneven_points(inputs, 6, 11, sizes=(1024, 4096), limb_range=(29, 80))
     cache = str(tmp_path / "tune.txt")
