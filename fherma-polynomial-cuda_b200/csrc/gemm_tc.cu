@@ -41,6 +41,7 @@ constexpr long long kTimeoutCycles = 4000000000ll;
 constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers, TMEM slot*/;
 
 __device__ uint32_t g_tc_error;
+__device__ uint32_t g_tile_counter;  // tile counter of GEMMs without one of their own
 
 // Instruction descriptor: D s32, A/B unsigned 8-bit, both K-major, M=128, N=256.
 constexpr uint32_t kInstrDesc = (2u << 4)              /* c_format = S32 */
@@ -136,6 +137,7 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&v)[32]) {
 struct TileShape {
     uint32_t m, columns, k_tiles, m_tiles, n_tiles, group_m;
     RowMap rows;
+    uint32_t* tile_counter;  // pair kernel: next unclaimed tile (zero at launch)
 };
 
 // Tile index -> (m tile, n tile) in groups of group_m m-tiles, m fastest, so the
@@ -452,6 +454,43 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait with cluster-scope acquire: data written by the other CTA of the pair before its
+// release-arrive on this barrier is visible afterwards.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) {
+    const long long start = clock64();
+    for (uint32_t i = 0;; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 255u) == 255u && clock64() - start > kTimeoutCycles) return false;
+    }
+}
+
+__device__ __forceinline__ uint32_t peer_address(const void* local) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(1));
+    return remote;
+}
+
+// Dynamic tile order: the leader's producer claims tile indices from a global counter (zeroed
+// by the host before the launch) and hands each one to every role of both CTAs through a ring
+// of kRing slots: tile_ring[slot] plus ring_full[slot] in each CTA, and ring_empty[slot] in the
+// leader, which all kRingReaders readers arrive on once they have read the slot. An index at or
+// past the tile count ends every role's loop. Claiming in order keeps the tiles in flight within
+// one window of the raster order (one L2-sized group), whatever the pace of each pair.
+constexpr uint32_t kRing = 4;
+constexpr uint32_t kRingReaders = 1 /* peer producer */ + 1 /* leader MMA */ + 2 * kEpilogueWarps;
+
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap a_map, const __grid_constant__ CUtensorMap b_map,
                         TileShape shape, Epilogue epi) {
@@ -464,13 +503,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     uint64_t* acc_full = empty + kPairStages;  // [2]
     uint64_t* acc_empty = acc_full + 2;        // [2] (leader's are used)
     uint64_t* drain = acc_empty + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    uint64_t* ring_full = drain + 1;           // [kRing]
+    uint64_t* ring_empty = ring_full + kRing;  // [kRing] (leader's are used)
+    uint32_t* tile_ring = reinterpret_cast<uint32_t*>(ring_empty + kRing);  // [kRing]
+    uint32_t* tmem_slot = tile_ring + kRing;
     volatile uint32_t* abort_flag = tmem_slot + 1;
 
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t rank = cluster_rank();
     const bool leader = rank == 0;
-    const uint32_t pair = blockIdx.x / 2, pairs = gridDim.x / 2;
     const uint32_t tiles = shape.m_tiles * shape.n_tiles;  // m_tiles counts 256-row pair tiles
 
     if (threadIdx.x == 0) {
@@ -481,6 +522,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         for (uint32_t a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
             mbar_init(&acc_empty[a], 2 * kEpilogueWarps);
+        }
+        for (uint32_t i = 0; i < kRing; ++i) {
+            mbar_init(&ring_full[i], 1);
+            mbar_init(&ring_empty[i], kRingReaders);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -496,13 +541,48 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     cluster_sync();  // barriers and TMEM of both CTAs ready before any cross-CTA traffic
     fence_after();
     const uint32_t tmem = *tmem_slot;
+    const uint32_t ring_release = leader_address(&ring_empty[0]);  // + slot * 8
+
+    // Reads ring slot i (every reader): the tile index, or `tiles` after a timeout.
+    auto read_ring = [&](uint32_t i, bool all_lanes_wait) -> uint32_t {
+        const uint32_t slot = i % kRing, round = i / kRing;
+        bool ok = true;
+        if (all_lanes_wait || lane == 0) ok = !*abort_flag && mbar_wait_cluster(&ring_full[slot], round & 1);
+        uint32_t tile = ok ? tile_ring[slot] : tiles;
+        if (!ok) {
+            *abort_flag = 1;
+            atomicOr(&g_tc_error, 256u);
+        }
+        return tile;
+    };
 
     if (warp == 0) {
         if (lane == 0) {
             // ---------------- TMA producer (both CTAs): own A half and B half, leader's barrier
             uint32_t step = 0;
             bool ok = true;
-            for (uint32_t tile = pair; tile < tiles && ok; tile += pairs) {
+            for (uint32_t i = 0; ok; ++i) {
+                uint32_t tile;
+                if (leader) {  // claim the next tile and publish it to both CTAs
+                    const uint32_t slot = i % kRing, round = i / kRing;
+                    if (*abort_flag || !mbar_wait_cluster(&ring_empty[slot], (round & 1) ^ 1)) {
+                        ok = false;
+                        // release every reader of this and later slots: they see an end index
+                        tile = tiles;
+                    } else {
+                        tile = atomicAdd(shape.tile_counter, 1u);
+                    }
+                    if (tile > tiles) tile = tiles;
+                    tile_ring[slot] = tile;
+                    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_address(&tile_ring[slot])), "r"(tile)
+                                 : "memory");
+                    mbar_arrive_cluster(peer_address(&ring_full[slot]));
+                    mbar_arrive_local(&ring_full[slot]);
+                } else {
+                    tile = read_ring(i, true);
+                    mbar_arrive_cluster(ring_release + (i % kRing) * sizeof(uint64_t));
+                }
+                if (tile >= tiles) break;
                 uint32_t m_tile, n_tile;
                 tile_coords(tile, shape, m_tile, n_tile);
                 const uint32_t row0 = m_tile * 256 + rank * kBlockM;
@@ -530,7 +610,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             // ---------------- MMA issuer (leader only)
             uint32_t step = 0, local = 0;
             bool ok = true;
-            for (uint32_t tile = pair; tile < tiles && ok; tile += pairs, ++local) {
+            for (uint32_t i = 0; ok; ++i, ++local) {
+                const uint32_t tile = read_ring(i, true);
+                mbar_arrive_local(&ring_empty[i % kRing]);
+                if (tile >= tiles) break;
                 const uint32_t acc = local & 1, use = local >> 1;
                 if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1)) {
                     ok = false;
@@ -566,8 +649,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         // ---------------- epilogue: this CTA's 128 rows of each pair tile
         const uint32_t quarter = warp & 3;
         const uint32_t release = leader_address(&acc_empty[0]);
-        uint32_t local = 0;
-        for (uint32_t tile = pair; tile < tiles; tile += pairs, ++local) {
+        for (uint32_t i = 0, local = 0;; ++i, ++local) {
+            uint32_t tile = read_ring(i, false);
+            tile = __shfl_sync(0xffffffffu, tile, 0);
+            if (lane == 0) {
+                if (leader)
+                    mbar_arrive_local(&ring_empty[i % kRing]);
+                else
+                    mbar_arrive_cluster(ring_release + (i % kRing) * sizeof(uint64_t));
+            }
+            if (tile >= tiles) break;
             const uint32_t acc = local & 1, use = local >> 1;
             uint32_t m_tile, n_tile;
             tile_coords(tile, shape, m_tile, n_tile);
@@ -709,6 +800,15 @@ bool prepare_gemm_tensor(TensorGemmPlan& plan, const uint8_t* a, uint64_t a_pitc
     plan.rows = rows;
     plan.a_tile_bytes = uint64_t(kBlockM) * k_bytes;
     plan.error_flag = tensor_gemm_error_flag();
+    if (!plan.tile_counter) {  // callers that keep GEMMs of one plan on one stream may bind their own
+        void* counter = nullptr;
+        if (cudaGetSymbolAddress(&counter, g_tile_counter) != cudaSuccess) {
+            cudaGetLastError();
+            why = "no tile counter";
+            return false;
+        }
+        plan.tile_counter = static_cast<uint32_t*>(counter);
+    }
     int device = 0, sms = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -737,11 +837,12 @@ void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cu
     // largest raster group whose A tiles fit comfortably in L2 (~48 MB)
     uint64_t group = (48ull << 20) / (plan.a_tile_bytes * (pairs ? 2 : 1));
     group = group < 4 ? 4 : (group > 64 ? 64 : group);
-    TileShape shape{m, plan.columns, plan.k_tiles, m_tiles, plan.n_tiles, uint32_t(group), rows};
+    TileShape shape{m, plan.columns, plan.k_tiles, m_tiles, plan.n_tiles, uint32_t(group), rows, plan.tile_counter};
     const uint32_t tiles = m_tiles * plan.n_tiles;
     if (pairs) {
         const uint32_t max_pairs = plan.sm_count / 2;
         const uint32_t grid = 2 * (tiles < max_pairs ? tiles : max_pairs);
+        cudaMemsetAsync(plan.tile_counter, 0, sizeof(uint32_t), stream);
         gemm_tc_pair_kernel<<<grid, kThreads, kPairSmemBytes, stream>>>(plan.a_map, plan.b_map_half, shape, epilogue);
         return;
     }

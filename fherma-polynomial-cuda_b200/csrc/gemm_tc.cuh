@@ -10,13 +10,15 @@
 namespace negacyclic {
 
 struct TensorGemmPlan {
-    CUtensorMap a_map;   // 3-D view of A: (K bytes, s, rows / s), box (128, 1, 128), 128B swizzle
+    CUtensorMap a_map;   // 2-D view of A: (K bytes, rows),          box (128, 128),   128B swizzle
     CUtensorMap b_map;   // 2-D view of B: (K bytes, columns),       box (128, 256),   128B swizzle
     CUtensorMap b_map_half;  // same view, box (128, 128): one CTA's half of a pair tile
     uint32_t m = 0, columns = 0, k_bytes = 0;
     uint32_t m_tiles = 0, n_tiles = 0, k_tiles = 0;
     RowMap rows{};
     uint32_t* error_flag = nullptr;  // device word set when a pipeline wait times out
+    uint32_t* tile_counter = nullptr;  // device word the CTA-pair kernel claims tiles from; GEMMs that
+                                       // share one may not run at the same time
     uint32_t sm_count = 148;          // persistent grid size
     uint64_t a_tile_bytes = 0;        // bytes of one 128-row A tile (raster group sizing)
     bool pairs = false;               // 2-CTA (cta_group::2) 256x256 tiles

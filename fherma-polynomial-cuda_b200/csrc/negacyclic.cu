@@ -138,7 +138,7 @@ void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cud
 
 // Work-space layout of one product (256-byte aligned pieces).
 struct WorkLayout {
-    size_t operands, residues, crt_in, dots, result, error_flag, total;
+    size_t operands, residues, crt_in, dots, result, error_flag, tile_counter, total;
 };
 
 WorkLayout work_layout(const negacyclic_plan& s) {
@@ -158,6 +158,8 @@ WorkLayout work_layout(const negacyclic_plan& s) {
     at = align(at + size_t(h.n) * h.limbs * 4);
     w.error_flag = at;
     at = align(at + 4);
+    w.tile_counter = at;  // the tensor-core GEMMs of this work space run one after another
+    at = align(at + 4);
     w.total = at;
     return w;
 }
@@ -176,6 +178,7 @@ std::string bind_work(negacyclic_plan& s, void* arena) {
     s.error_flag = reinterpret_cast<uint32_t*>(base + w.error_flag);
     s.convert_engine = s.crt_engine = NEGACYCLIC_GEMM_SIMT;
     if (!s.gemm_tensor_wanted) return "";
+    s.convert_gemm.tile_counter = s.crt_gemm.tile_counter = reinterpret_cast<uint32_t*>(base + w.tile_counter);
     std::string why_convert, why_crt;
     if (prepare_gemm_tensor(s.convert_gemm, reinterpret_cast<const uint8_t*>(s.operands), uint64_t(s.padded_limbs) * 4,
                             RowMap::split_rows(h.n, h.n_sub, h.split, 0, h.n_sub, 0, h.split), 2 * h.n, s.convert_weights,
