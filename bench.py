@@ -41,6 +41,10 @@ N, LIMBS, SEED = 65536, 1747, 2
 METRIC = "products/s at N=65536,W=1747 (limbs)"
 WORKLOAD = "negacyclic product N=65536, L=1747 limbs (55904-bit random odd q, seed 2), a,b uniform in [0,q)"
 CPU_SAMPLE_N = N // 32  # bounded CPU sample: 2048 coefficients of the same width
+# DRAM bytes (read + write) of one conversion-GEMM launch on this workload, from a one-pass ncu
+# capture (dram__bytes_read.sum 4.33 GB + dram__bytes_write.sum 1.90 GB) of
+#   python bench.py --workload 65536,1747 --steps 1 --warmup 1 --device-only
+CONVERT_DRAM_BYTES = 6.23e9
 
 
 def _load(name, path, package_dir=None):
@@ -273,10 +277,16 @@ def run_b200(args):
     conv_ops = 2.0 * (2 * n_coeff) * (4 * limbs) * (4 * info["primes"])
     crt_ops = 2.0 * n_coeff * (4 * info["primes"]) * (4 * info["words"])
     conv_tops = conv_ops / (stage_ms["convert"] / 1000) / 1e12
+    padded_limbs = (limbs + 31) // 32 * 32
     roofline = {
         "bound": "tensor", "kernel": "gemm_tc_kernel (conversion, tcgen05 kind::i8)",
         "achieved": round(conv_tops, 1), "peak": round(int8_peak, 1), "unit": "TOPS (int8)",
-        "frac": round(conv_tops / int8_peak, 4), "traffic": None,
+        "frac": round(conv_tops / int8_peak, 4),
+        "traffic": CONVERT_DRAM_BYTES if (n_coeff, limbs) == (N, LIMBS) else None,
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+        # operand rows (padded to 32 limbs), conversion weights, residues written
+        "algorithmic_bytes_per_launch": float(2 * n_coeff * 4 * padded_limbs + 4 * info["padded_primes"] * 4 * padded_limbs
+                                              + 2 * info["primes"] * n_coeff * 4),
         "peak_source": f"2 x bf16 dense, {source}: {bf16_tflops} TF/s",
         "algorithmic_ops_per_launch": conv_ops,
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
