@@ -274,7 +274,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         // host products stream in transform-ordered chunks (max(8, s) of them) once each chunk
         // keeps 128-row GEMM tiles
         s.chunks = (h.n_sub >= 1024 && h.n >= 8192) ? std::max(8u, h.split) : 1;
-        for (uint32_t c = 0; c < s.chunks; ++c) {
+        for (uint32_t c = 0; c < (s.chunks > 1 ? negacyclic_plan::kMaxChunks : 1u); ++c) {
             check(cudaEventCreateWithFlags(&s.in_ready[c], cudaEventDisableTiming), "cudaEventCreate");
             check(cudaEventCreateWithFlags(&s.out_ready[c], cudaEventDisableTiming), "cudaEventCreate");
             check(cudaEventCreateWithFlags(&s.copied_out[c], cudaEventDisableTiming), "cudaEventCreate");
@@ -454,20 +454,63 @@ void ensure_staging(negacyclic_plan& s) {
     }
 }
 
-// Streamed host products run in s.chunks chunks each way.
-// In: rows of at least 1 KB go in transform order: chunk c is transform t = c / parts, positions
-// j in [j0, j0 + span), i.e. coefficients s*j + t (one 2-D copy per operand), so the forward NTTs
+// Streamed host products run in about max(8, s) chunks each way (stream_chunks below).
+// In: rows of at least 1 KB go in transform order: a chunk is part of transform t, positions j
+// in [j0, j0 + span), i.e. coefficients s*j + t (one 2-D copy per operand), so the forward NTTs
 // of transform t run while later transforms are still being copied in. Narrower rows go as
 // contiguous coefficient ranges, whose forward NTTs wait for the last chunk.
 // Out: contiguous coefficient ranges; each chunk's copy-out overlaps the next chunk's CRT GEMM
 // and reduction.
-struct Chunk {
+struct InChunk {  // transform t, positions j in [j0, j0 + span): coefficients s*j + t
     uint32_t t, j0, span;
 };
+struct OutChunk {  // coefficients [first, first + count)
+    uint32_t first, count;
+};
 
-Chunk chunk_of(const negacyclic_plan& s, uint32_t c) {
-    const uint32_t parts = s.chunks / s.host.split, span = s.host.n_sub / parts;
-    return Chunk{c / parts, (c % parts) * span, span};
+bool transform_ordered_input(const negacyclic_plan& s);
+
+// Chunk lists of a streamed host product (at most kMaxChunks each way).
+// In, transform-ordered: `parts` chunks per transform, the last transform cut finer, so that
+// little conversion is left once the link has delivered everything. In, coefficient-ordered:
+// equal coefficient ranges, the last one cut in four. Out: coefficient ranges growing from a
+// quarter of a chunk, so the copy-out starts soon after the last inverse NTT.
+void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vector<OutChunk>& out) {
+    const HostPlan& h = s.host;
+    const uint32_t split = h.split, n_sub = h.n_sub, per = h.n / s.chunks;
+    constexpr uint32_t kMax = negacyclic_plan::kMaxChunks;
+    in.clear();
+    out.clear();
+    if (s.chunks == 1) {  // small product: one piece each way
+        in.push_back(InChunk{0, 0, h.n});
+        out.push_back(OutChunk{0, h.n});
+        return;
+    }
+    if (transform_ordered_input(s)) {
+        const uint32_t parts = s.chunks / split;
+        uint32_t tail = parts;  // power of two, spans of >= 256 rows, within the event budget
+        while (tail * 2 <= 4 * parts && (split - 1) * parts + tail * 2 <= kMax && n_sub / (tail * 2) >= 256) tail *= 2;
+        for (uint32_t t = 0; t < split; ++t) {
+            const uint32_t p = t + 1 == split ? tail : parts, span = n_sub / p;
+            for (uint32_t k = 0; k < p; ++k) in.push_back(InChunk{t, k * span, span});
+        }
+    } else {
+        const uint32_t quarter = per / 4;
+        const bool cut = quarter / split >= 256 && s.chunks + 3 <= kMax;
+        for (uint32_t k = 0; k + 1 < s.chunks; ++k) in.push_back(InChunk{0, k * per, per});
+        if (cut)
+            for (uint32_t k = 0; k < 4; ++k) in.push_back(InChunk{0, (s.chunks - 1) * per + k * quarter, quarter});
+        else
+            in.push_back(InChunk{0, (s.chunks - 1) * per, per});
+    }
+    // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
+    uint32_t first = 0, size = (per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
+    for (uint32_t k = 0; first < h.n; ++k) {
+        const uint32_t count = std::min(size, h.n - first);
+        out.push_back(OutChunk{first, count});
+        first += count;
+        if (k >= 1 && size < per) size *= 2;  // per/4, per/4, per/2, per, per, ...
+    }
 }
 
 bool transform_ordered_input(const negacyclic_plan& s) {
@@ -488,7 +531,7 @@ void copy_rows_async(void* dst, size_t dpitch, const void* src, size_t spitch, s
 void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     const HostPlan& h = s.host;
     const size_t row = size_t(h.limbs) * 4, words = size_t(h.n) * h.limbs;
-    const uint32_t split = h.split, n_sub = h.n_sub, chunks = s.chunks, per = h.n / chunks;
+    const uint32_t split = h.split, n_sub = h.n_sub;
     cudaStream_t st = s.stream;
     const bool a_locked = page_locked(a), b_locked = page_locked(b);
     s.outputs_staged = !(c && page_locked(c));
@@ -499,12 +542,14 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     // rows land unpadded (straight in the operands when they need neither padding nor
     // permutation) and are padded on the device; the CRT word-sum buffer, written only after
     // every chunk is converted, stages them
+    std::vector<InChunk> in;
+    std::vector<OutChunk> out;
+    stream_chunks(s, in, out);
     if (transform_ordered_input(s)) {
         const bool direct = s.padded_limbs == h.limbs;
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
-        const uint32_t parts = chunks / split;
-        for (uint32_t k = 0; k < chunks; ++k) {
-            const Chunk ch = chunk_of(s, k);
+        for (uint32_t k = 0; k < in.size(); ++k) {
+            const InChunk ch = in[k];
             const size_t host_row0 = size_t(split) * ch.j0 + ch.t, buf_row0 = size_t(ch.t) * n_sub + ch.j0;
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + host_row0 * h.limbs;
@@ -523,14 +568,14 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
             if (!direct)
                 launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, 1, uint32_t(buf_row0), ch.span, st);
             enqueue_convert(s, ch.t, 1, ch.j0, ch.span, st);
-            if (k % parts == parts - 1)  // transform t complete: its forward NTTs, both operands
+            if (k + 1 == in.size() || in[k + 1].t != ch.t)  // transform t complete: its forward NTTs
                 launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, ch.t, 1, st);
         }
     } else {
         const bool direct = s.padded_limbs == h.limbs && split == 1;
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
-        for (uint32_t k = 0; k < chunks; ++k) {
-            const size_t first = size_t(k) * per, bytes = size_t(per) * row;
+        for (uint32_t k = 0; k < in.size(); ++k) {
+            const size_t first = in[k].j0, count = in[k].span, bytes = count * row;  // coefficient range
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + first * h.limbs;
                 if (!locked[op]) {
@@ -544,9 +589,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
             check(cudaEventRecord(s.in_ready[k], s.copy_in), "cudaEventRecord");
             check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
             if (!direct)
-                launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, split, uint32_t(first), per, st);
-            const uint32_t span = n_sub / chunks;  // coefficients [first, first + per): j in [k span, (k+1) span)
-            enqueue_convert(s, 0, split, k * span, span, st);
+                launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, split, uint32_t(first),
+                                uint32_t(count), st);
+            // coefficients [first, first + count): j in [first / s, (first + count) / s) of every transform
+            enqueue_convert(s, 0, split, uint32_t(first / split), uint32_t(count / split), st);
         }
         launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, 0, split, st);
     }
@@ -555,15 +601,15 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, 0, h.n, st);
     // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
     uint32_t* dst = s.outputs_staged ? s.stage_out : c;
-    for (uint32_t k = 0; k <= chunks; ++k) {
-        if (k < chunks) {
-            enqueue_output(s, k * per, per, s.result, st);
+    for (uint32_t k = 0; k <= out.size(); ++k) {
+        if (k < out.size()) {
+            enqueue_output(s, out[k].first, out[k].count, s.result, st);
             check(cudaEventRecord(s.out_ready[k], st), "cudaEventRecord");
         }
         if (k >= 1) {
-            const size_t first = size_t(k - 1) * per;
+            const size_t first = out[k - 1].first;
             check(cudaStreamWaitEvent(s.copy_out, s.out_ready[k - 1], 0), "cudaStreamWaitEvent");
-            check(cudaMemcpyAsync(dst + first * h.limbs, s.result + first * h.limbs, size_t(per) * row,
+            check(cudaMemcpyAsync(dst + first * h.limbs, s.result + first * h.limbs, size_t(out[k - 1].count) * row,
                                   cudaMemcpyDeviceToHost, s.copy_out),
                   "copy c");
             check(cudaEventRecord(s.copied_out[k - 1], s.copy_out), "cudaEventRecord");
@@ -575,12 +621,14 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
 // Waits for a host product; copies staged output chunks into c as they land.
 int host_finish(negacyclic_plan& s, uint32_t* c) {
     const HostPlan& h = s.host;
-    const uint32_t chunks = s.chunks, per = h.n / chunks;
     if (s.outputs_staged) {
-        for (uint32_t k = 0; k < chunks; ++k) {
+        std::vector<InChunk> in;
+        std::vector<OutChunk> out;
+        stream_chunks(s, in, out);
+        for (uint32_t k = 0; k < out.size(); ++k) {
             check(cudaEventSynchronize(s.copied_out[k]), "copy c");
-            const size_t first = size_t(k) * per;
-            s.team->copy(c + first * h.limbs, s.stage_out + first * h.limbs, size_t(per) * h.limbs * 4);
+            const size_t first = out[k].first;
+            s.team->copy(c + first * h.limbs, s.stage_out + first * h.limbs, size_t(out[k].count) * h.limbs * 4);
         }
     }
     uint32_t flag = 0, pipeline = 0;
@@ -621,7 +669,7 @@ int negacyclic_prepare_host(negacyclic_plan* s) {
         const size_t words = size_t(s->host.n) * s->host.limbs;
         std::memset(s->stage_in, 0, 2 * words * 4);
         host_begin(*s, s->stage_in, s->stage_in + words, nullptr);
-        for (uint32_t k = 0; k < s->chunks; ++k) check(cudaEventSynchronize(s->copied_out[k]), "warm-up");
+        check(cudaStreamSynchronize(s->copy_out), "warm-up");
         check(cudaStreamSynchronize(s->stream), "warm-up");
         uint32_t flag = 0;
         check(cudaMemcpy(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost), "warm-up");

@@ -174,6 +174,25 @@ def test_run_device_matches_run(fpc, inputs, torch):
             assert np.array_equal(dc.cpu().numpy().view(np.uint32), host)
 
 
+@pytest.mark.parametrize("limbs", [300, 100])  # 1200-byte rows: transform-ordered input; 400-byte: by coefficient
+def test_streamed_host_path_with_sixteen_transforms(limbs, fpc, inputs, oracle, torch):
+    """s = 16 gives 16 input chunks (the event budget) and the plain output split; the host path
+    must equal the unchunked device path, and spot coefficients the schoolbook sums."""
+    n = 65536
+    q, a, b = inputs.instance(n, limbs, 31, 0)
+    with fpc.Plan(n, 32 * limbs, limbs, q, split=16) as plan:
+        assert plan.info()["split"] == 16
+        host = plan.run(a, b)
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(b.view(np.int32)).cuda()
+        dc = torch.empty_like(da)
+        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(dc.cpu().numpy().view(np.uint32), host)
+    for i in (0, 1, 15, 16, 4097, n - 1):
+        assert np.array_equal(oracle.schoolbook_at(q, a, b, i)[0], host[i]), i
+
+
 # ---------------------------------------------------------------- full-size configurations
 
 def big_points():
