@@ -435,23 +435,26 @@ __global__ void pointwise_kernel(uint32_t* residues, const DevicePrime* __restri
     }
 }
 
-// residues[0][k][rho] -> crt_in[s*j + v][k] for rho = v*N' + j in [first, first + count) (coefficient
-// s*j + v, coefficient-major); zero for k in [r, r').
+// residues[0][k][v*N' + j] -> crt_in[s*j + v][k] (coefficient-major) for every transform v and
+// j in [j_first, j_first + j_count), i.e. coefficients [s j_first, s (j_first + j_count)); zero for
+// k in [r, r'). Block x covers up to 32 consecutive j of one transform.
 __global__ void transpose_kernel(const uint32_t* __restrict__ residues, uint32_t* __restrict__ crt_in,
                                  uint32_t r, uint32_t padded_r, uint32_t n, uint32_t log_split, uint32_t log_n_sub,
-                                 uint32_t first, uint32_t count) {
+                                 uint32_t j_first, uint32_t j_count) {
     __shared__ uint32_t tile[32][33];
-    const uint32_t rho0 = first + blockIdx.x * 32, k0 = blockIdx.y * 32, end = first + count;
-    const uint32_t x = threadIdx.x, y = threadIdx.y, n_sub_mask = (1u << log_n_sub) - 1;
+    const uint32_t blocks_per_v = (j_count + 31) / 32, v = blockIdx.x / blocks_per_v;
+    const uint32_t j0 = j_first + (blockIdx.x - v * blocks_per_v) * 32, k0 = blockIdx.y * 32;
+    const uint32_t j_end = j_first + j_count, rho0 = (v << log_n_sub) + j0;
+    const uint32_t x = threadIdx.x, y = threadIdx.y;
     for (uint32_t dy = 0; dy < 32; dy += 8) {
-        uint32_t k = k0 + y + dy, rho = rho0 + x;
-        tile[y + dy][x] = (k < r && rho < end) ? residues[size_t(k) * n + rho] : 0u;
+        uint32_t k = k0 + y + dy;
+        tile[y + dy][x] = (k < r && j0 + x < j_end) ? residues[size_t(k) * n + rho0 + x] : 0u;
     }
     __syncthreads();
     for (uint32_t dy = 0; dy < 32; dy += 8) {
-        uint32_t rho = rho0 + y + dy, k = k0 + x;
-        if (rho >= end || k >= padded_r) continue;
-        const size_t coefficient = (size_t(rho & n_sub_mask) << log_split) + (rho >> log_n_sub);
+        uint32_t j = j0 + y + dy, k = k0 + x;
+        if (k >= padded_r || j >= j_end) continue;
+        const size_t coefficient = (size_t(j) << log_split) + v;
         crt_in[coefficient * padded_r + k] = tile[x][y + dy];
     }
 }
@@ -730,11 +733,11 @@ void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2
 }
 
 void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r, uint32_t n,
-                      uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream) {
+                      uint32_t split, uint32_t j_first, uint32_t j_count, cudaStream_t stream) {
     const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
-    dim3 grid((count + 31) / 32, padded_r / 32);
-    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, log_split, log_n_sub, first,
-                                                       count);
+    dim3 grid(split * ((j_count + 31) / 32), padded_r / 32);
+    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, log_split, log_n_sub,
+                                                       j_first, j_count);
 }
 
 void launch_reduce(const ReduceParams& params, cudaStream_t stream) {

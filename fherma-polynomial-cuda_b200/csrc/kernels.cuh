@@ -96,10 +96,10 @@ void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2
 // inverse NTTs of transforms [v_first, v_first + v_count), every prime
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r,
                         uint32_t n, uint32_t n_sub, uint32_t v_first, uint32_t v_count, cudaStream_t stream);
-// crt_in[s*j + v][k] = residues[0][k][v*N' + j] for rho = v*N' + j in [first, first + count);
-// zero for k in [r, r')
+// crt_in[s*j + v][k] = residues[0][k][v*N' + j] for every v and j in [j_first, j_first + j_count):
+// coefficients [s j_first, s (j_first + j_count)); zero for k in [r, r')
 void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r,
-                      uint32_t n, uint32_t split, uint32_t first, uint32_t count, cudaStream_t stream);
+                      uint32_t n, uint32_t split, uint32_t j_first, uint32_t j_count, cudaStream_t stream);
 
 struct ReduceParams {
     const uint64_t* dots;     // [n][words]

@@ -120,7 +120,7 @@ void enqueue_middle(negacyclic_plan& s, cudaStream_t stream, cudaEvent_t* marks)
     mark();
     launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, n, h.n_sub, 0, h.split, stream);
     mark();
-    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, n, h.split, 0, n, stream);
+    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, n, h.split, 0, h.n_sub, stream);
     mark();
 }
 
@@ -470,6 +470,10 @@ struct OutChunk {  // coefficients [first, first + count)
 
 bool transform_ordered_input(const negacyclic_plan& s);
 
+// Rows of at least 1 KB: chunks carry enough work that finer chunks near the ends (and one
+// transpose per output chunk) pay for their extra launches. Narrower rows keep equal chunks.
+bool wide_rows(const negacyclic_plan& s) { return s.host.limbs >= 256; }
+
 // Chunk lists of a streamed host product (at most kMaxChunks each way).
 // In, transform-ordered: `parts` chunks per transform, the last transform cut finer, so that
 // little conversion is left once the link has delivered everything. In, coefficient-ordered:
@@ -496,7 +500,7 @@ void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vect
         }
     } else {
         const uint32_t quarter = per / 4;
-        const bool cut = quarter / split >= 256 && s.chunks + 3 <= kMax;
+        const bool cut = wide_rows(s) && quarter / split >= 256 && s.chunks + 3 <= kMax;
         for (uint32_t k = 0; k + 1 < s.chunks; ++k) in.push_back(InChunk{0, k * per, per});
         if (cut)
             for (uint32_t k = 0; k < 4; ++k) in.push_back(InChunk{0, (s.chunks - 1) * per + k * quarter, quarter});
@@ -504,7 +508,7 @@ void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vect
             in.push_back(InChunk{0, (s.chunks - 1) * per, per});
     }
     // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
-    uint32_t first = 0, size = (per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
+    uint32_t first = 0, size = (wide_rows(s) && per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
     for (uint32_t k = 0; first < h.n; ++k) {
         const uint32_t count = std::min(size, h.n - first);
         out.push_back(OutChunk{first, count});
@@ -514,7 +518,7 @@ void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vect
 }
 
 bool transform_ordered_input(const negacyclic_plan& s) {
-    return s.chunks > 1 && s.host.split > 1 && s.host.limbs >= 256;  // chunks >= split when chunked
+    return s.chunks > 1 && s.host.split > 1 && wide_rows(s);  // chunks >= split when chunked
 }
 
 void copy_rows_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row, uint32_t rows,
@@ -598,11 +602,17 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     }
     launch_pointwise(s.residues, s.primes, s.zeta, s.r, h.n, n_sub, split, st);
     launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, h.n, n_sub, 0, split, st);
-    launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, 0, h.n, st);
-    // outputs: CRT GEMM + reduction per chunk, each chunk's copy-out overlapping the next chunk
+    // outputs: CRT GEMM and reduction per chunk, each chunk's copy-out overlapping the next
+    // chunk's work. With wide rows the transpose also goes chunk by chunk, so only the first
+    // chunk's share sits between the inverse NTT and the first copy-out.
     uint32_t* dst = s.outputs_staged ? s.stage_out : c;
+    const bool transpose_per_chunk = wide_rows(s);
+    if (!transpose_per_chunk) launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, 0, n_sub, st);
     for (uint32_t k = 0; k <= out.size(); ++k) {
         if (k < out.size()) {
+            if (transpose_per_chunk)  // chunk coefficients are whole multiples of s
+                launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, out[k].first / split,
+                                 out[k].count / split, st);
             enqueue_output(s, out[k].first, out[k].count, s.result, st);
             check(cudaEventRecord(s.out_ready[k], st), "cudaEventRecord");
         }
