@@ -199,6 +199,48 @@ def big_points():
     return [p for p in baseline_points() if p["N"] * p["L"] > 4096 * 64]
 
 
+def _constant(x):
+    """The common value of a polynomial whose coefficients are all equal, else None."""
+    return int.from_bytes(x[0].astype("<u4").tobytes(), "little") if (x == x[0]).all() else None
+
+
+@pytest.mark.parametrize("point", big_points(), ids=lambda p: f"N{p['N']}_L{p['L']}")
+def test_full_size_edge_inputs(point, fpc, inputs, oracle):
+    """Every edge pair of the reference's checks (zero, unit, all q-1, impulses at 0 and N-1,
+    alternating q-1/q-2, 0xFFFFFFFF limbs below q, limb boundaries, q/2) at N=32768/L=868 and
+    N=65536/L=1747, checked exactly without a full GMP product:
+      constant a, b:       c_i = a b (2i + 2 - N) mod q (negacyclic sum of N equal terms)
+      impulses:            one nonzero coefficient, at the shifted index
+      q-1 at odd j, ones:  c_i = (q-1) (2 floor((i+1)/2) - N/2) mod q
+      others:              direct coefficient sums (schoolbook) at spot indices."""
+    n, limbs, seed = point["N"], point["L"], point["seed"]
+    q = inputs.random_modulus(limbs, seed)
+    qi = inputs.to_int(q)
+    edges = inputs.edge_operands(n, q)
+    with fpc.Plan(n, 32 * limbs, limbs, q) as plan:
+        for x, y in inputs.EDGE_PAIRS:
+            a, b = edges[x], edges[y]
+            c = plan.run(a, b)
+            got = inputs.poly_to_ints(c)
+            ca, cb = _constant(a), _constant(b)
+            if ca is not None and cb is not None:
+                base = ca * cb % qi
+                want = [base * (2 * i + 2 - n) % qi for i in range(n)]
+            elif (x, y) == ("impulse0", "impulse_last"):  # 1 * (q-1) X^(N-1)
+                want = [0] * n
+                want[n - 1] = qi - 1
+            elif (x, y) == ("impulse_last", "impulse_last"):  # (q-1)^2 X^(2N-2) = -X^(N-2)
+                want = [0] * n
+                want[n - 2] = qi - 1
+            elif (x, y) == ("alt_zero", "ones"):
+                want = [(qi - 1) * (2 * ((i + 1) // 2) - n // 2) % qi for i in range(n)]
+            else:
+                for i in (0, n // 2 + 1, n - 1):
+                    assert np.array_equal(oracle.schoolbook_at(q, a, b, i)[0], c[i]), (x, y, i)
+                continue
+            assert got == want, (x, y)
+
+
 @pytest.mark.parametrize("point", big_points(), ids=lambda p: f"N{p['N']}_L{p['L']}")
 def test_full_size_against_reference_hash_and_properties(point, fpc, inputs, oracle):
     """Bit-exact at N=32768/L=868 and N=65536/L=1747 against the reference checker's hash,
