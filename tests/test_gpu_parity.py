@@ -242,6 +242,29 @@ def test_full_size_edge_inputs(point, fpc, inputs, oracle):
 
 
 @pytest.mark.parametrize("point", big_points(), ids=lambda p: f"N{p['N']}_L{p['L']}")
+def test_full_size_seeded_instances(point, fpc, inputs, oracle):
+    """Further seeded instances of the full-size configurations, checked through exact
+    properties: a b = b a, (a1 + a2) b = a1 b + a2 b (mod q), and direct coefficient sums at
+    one index each."""
+    n, limbs, seed = point["N"], point["L"], point["seed"]
+    q = inputs.random_modulus(limbs, seed)
+    qi = inputs.to_int(q)
+    instances = [inputs.instance(n, limbs, seed, index)[1:] for index in range(1, 4)]
+    with fpc.Plan(n, 32 * limbs, limbs, q) as plan:
+        products = [plan.run(a, b) for a, b in instances]
+        (a1, b1), (a2, _), _ = instances
+        assert np.array_equal(plan.run(b1, a1), products[0])
+        a12 = inputs.poly_from_ints([(x + y) % qi for x, y in zip(inputs.poly_to_ints(a1), inputs.poly_to_ints(a2))],
+                                    limbs)
+        sum_product = inputs.poly_to_ints(plan.run(a12, b1))
+        a2b1 = inputs.poly_to_ints(plan.run(a2, b1))
+    c1 = inputs.poly_to_ints(products[0])
+    assert sum_product == [(x + y) % qi for x, y in zip(c1, a2b1)]
+    for (a, b), c, i in zip(instances, products, (1, n // 3, n - 2)):
+        assert np.array_equal(oracle.schoolbook_at(q, a, b, i)[0], c[i]), i
+
+
+@pytest.mark.parametrize("point", big_points(), ids=lambda p: f"N{p['N']}_L{p['L']}")
 def test_full_size_against_reference_hash_and_properties(point, fpc, inputs, oracle):
     """Bit-exact at N=32768/L=868 and N=65536/L=1747 against the reference checker's hash,
     plus size-independent checks: direct coefficient sums, and a*(X b) = X (a b)."""
