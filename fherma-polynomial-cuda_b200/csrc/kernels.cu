@@ -556,20 +556,35 @@ __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
         const uint64_t low = x0 + (x1 << 32);
         const uint64_t high = (x1 >> 32) + x2 + (low < x0 ? 1 : 0);  // D = high 2^64 + low
         const uint64_t kq = high + ((low + (1ull << 63)) < low ? 1 : 0);
-        // 2. T' = sum_w (d[w] + K R[w]) 2^(32w), collapsed to exact words in one carry pass
+        // 2. T' = sum_w (d[w] + K R[w]) 2^(32w), collapsed to exact words in one carry pass.
+        //    The word sums come from DRAM: kBatch steps' worth are loaded before any is used, so
+        //    one load latency covers kBatch 32-word steps of the (serial) carry chain.
+        constexpr uint32_t kBatch = 8;
         uint32_t chain = 0, carried_high = 0;
-        for (uint32_t base = 0; base < tlen; base += 32) {
-            const uint32_t w = base + lane;
-            uint64_t value = 0;
-            if (w < tlen) value = d[w] + (w < limbs ? kq * prm.minus_p[w] : 0ull);
-            const uint32_t high32 = uint32_t(value >> 32);
-            uint32_t below = __shfl_up_sync(kFull, high32, 1);
-            if (lane == 0) below = carried_high;
-            carried_high = __shfl_sync(kFull, high32, 31);
-            const uint64_t sum = uint64_t(uint32_t(value)) + below;
-            const uint32_t word = uint32_t(sum);
-            const uint32_t carry = chain_carry((sum >> 32) != 0, word == kFull, chain);
-            if (w < tlen) v[w] = word + carry;
+        for (uint32_t batch = 0; batch < tlen; batch += 32 * kBatch) {
+            uint64_t loaded[kBatch];
+            uint32_t r_words[kBatch];
+#pragma unroll
+            for (uint32_t u = 0; u < kBatch; ++u) {
+                const uint32_t w = batch + 32 * u + lane;
+                loaded[u] = w < tlen ? d[w] : 0ull;
+                r_words[u] = w < limbs ? prm.minus_p[w] : 0u;
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kBatch; ++u) {
+                const uint32_t base = batch + 32 * u;
+                if (base >= tlen) break;  // warp-uniform
+                const uint32_t w = base + lane;
+                const uint64_t value = loaded[u] + kq * r_words[u];  // both zero past the end
+                const uint32_t high32 = uint32_t(value >> 32);
+                uint32_t below = __shfl_up_sync(kFull, high32, 1);
+                if (lane == 0) below = carried_high;
+                carried_high = __shfl_sync(kFull, high32, 31);
+                const uint64_t sum = uint64_t(uint32_t(value)) + below;
+                const uint32_t word = uint32_t(sum);
+                const uint32_t carry = chain_carry((sum >> 32) != 0, word == kFull, chain);
+                if (w < tlen) v[w] = word + carry;
+            }
         }
         __syncwarp();
         // 3. Barrett quotient from the 128 bits of T' at q's top-64-bit window
