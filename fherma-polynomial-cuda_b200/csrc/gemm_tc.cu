@@ -163,13 +163,27 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& epi, const uint32
             if (c_base + j < columns) out[c_base + j] = int32_t(v[j]);
         return;
     }
+    uint64_t sum[8];
 #pragma unroll
-    for (int g = 0; g < 8; ++g) {
-        const uint32_t group_index = c_base / 4 + g;
-        const uint64_t s = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
-                           (uint64_t(v[4 * g + 3]) << 24);
-        if (group_index < epi.words) epi.dots[out_row * epi.words + group_index] = s;
+    for (int g = 0; g < 8; ++g)
+        sum[g] = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
+                 (uint64_t(v[4 * g + 3]) << 24);
+    // the lane's 8 words are consecutive in its row: whole 32-byte sectors when the row stride
+    // allows (the work space is 256-byte aligned, the chunk starts at a multiple of 8 words)
+    const uint32_t g0 = c_base / 4;
+    uint64_t* out = epi.dots + out_row * epi.words + g0;
+    if (g0 + 8 <= epi.words && (epi.words & 3) == 0) {
+        asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(out), "l"(sum[0]), "l"(sum[1]), "l"(sum[2]),
+                     "l"(sum[3])
+                     : "memory");
+        asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(out + 4), "l"(sum[4]), "l"(sum[5]),
+                     "l"(sum[6]), "l"(sum[7])
+                     : "memory");
+        return;
     }
+#pragma unroll
+    for (int g = 0; g < 8; ++g)
+        if (g0 + g < epi.words) out[g] = sum[g];
 }
 
 // One epilogue warp's share of an accumulator: 32 rows (one per lane) x 256 columns starting at
