@@ -168,11 +168,12 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& epi, const uint32
     for (int g = 0; g < 8; ++g)
         sum[g] = uint64_t(v[4 * g]) + (uint64_t(v[4 * g + 1]) << 8) + (uint64_t(v[4 * g + 2]) << 16) +
                  (uint64_t(v[4 * g + 3]) << 24);
-    // the lane's 8 words are consecutive in its row: whole 32-byte sectors when the row stride
-    // allows (the work space is 256-byte aligned, the chunk starts at a multiple of 8 words)
+    // the lane's 8 words are consecutive in its row: two whole 32-byte sectors (the work space is
+    // 256-byte aligned, rows are a multiple of 8 words, the chunk starts at a multiple of 8 words)
     const uint32_t g0 = c_base / 4;
-    uint64_t* out = epi.dots + out_row * epi.words + g0;
-    if (g0 + 8 <= epi.words && (epi.words & 3) == 0) {
+    if (g0 >= epi.words) return;
+    uint64_t* out = epi.dots + out_row * epi.dots_stride + g0;
+    if (g0 + 8 <= epi.dots_stride && (epi.dots_stride & 3) == 0) {
         asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(out), "l"(sum[0]), "l"(sum[1]), "l"(sum[2]),
                      "l"(sum[3])
                      : "memory");

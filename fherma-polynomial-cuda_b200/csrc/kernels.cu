@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restric
             rows.residue(m, op, column);
             epi.residues[(size_t(op) * epi.r + group) * epi.n + column] = redc(s, f.p, f.pinv);
         } else {
-            if (group < epi.words) epi.dots[rows.row(m) * epi.words + group] = s;
+            if (group < epi.words) epi.dots[rows.row(m) * epi.dots_stride + group] = s;
         }
     }
 }
@@ -547,10 +547,10 @@ __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x & 31;
     const uint32_t warps = blockDim.x / 32;
     uint32_t* v = scratch + size_t(warp) * stride;
-    const uint32_t words = prm.words, limbs = prm.limbs, tlen = limbs + 2;
+    const uint32_t limbs = prm.limbs, tlen = limbs + 2;
     const uint32_t* q = prm.q;
     for (uint32_t i = blockIdx.x * warps + warp; i < prm.n; i += gridDim.x * warps) {
-        const uint64_t* d = prm.dots + size_t(i) * words;
+        const uint64_t* d = prm.dots + size_t(i) * prm.dots_stride;
         // 1. K = (D + 2^63) >> 64, D = d[L+2] + d[L+3] 2^32 + d[L+4] 2^64 (each word sum < 2^56)
         const uint64_t x0 = d[limbs + 2], x1 = d[limbs + 3], x2 = d[limbs + 4];
         const uint64_t low = x0 + (x1 << 32);

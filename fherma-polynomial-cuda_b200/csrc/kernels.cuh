@@ -66,9 +66,10 @@ struct Epilogue {
     uint32_t* residues;
     const DevicePrime* primes;
     uint32_t r, n;
-    // crt: dots[row * words + g] = S (u64), g < words, row = the operand row of GEMM row m
+    // crt: dots[row * dots_stride + g] = S (u64), g < words, row = the operand row of GEMM row m;
+    //      dots_stride is words rounded up to a multiple of 8 (64-byte rows)
     uint64_t* dots;
-    uint32_t words;
+    uint32_t words, dots_stride;
 };
 
 // a, b: [N][L] -> out: [2][N][Lp], rows split-major (coefficient s*j + t at row op*N + t*N' + j),
@@ -102,11 +103,11 @@ void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, ui
                       uint32_t n, uint32_t split, uint32_t j_first, uint32_t j_count, cudaStream_t stream);
 
 struct ReduceParams {
-    const uint64_t* dots;     // [n][words]
+    const uint64_t* dots;     // [n][dots_stride], words used
     uint32_t* out;            // [n][limbs]
     const uint32_t* q;        // [limbs]
     const uint32_t* minus_p;  // [limbs]  (-P) mod q
-    uint32_t n, limbs, words;
+    uint32_t n, limbs, words, dots_stride;
     int32_t top_shift;
     uint64_t mu_low;
     uint32_t* error_flag;     // set nonzero if a coefficient needed more corrections than proven

@@ -84,6 +84,7 @@ void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t
     crt.mode = kEpilogueCrt;
     crt.dots = s.dots;
     crt.words = h.words;
+    crt.dots_stride = s.dots_stride;
     const RowMap rows = RowMap::linear(first);
     if (s.crt_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.crt_gemm, rows, count))
         launch_gemm_tensor(s.crt_gemm, crt, stream, rows, count);
@@ -92,7 +93,8 @@ void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t
                          s.crt_weights, s.crt_columns, s.k_crt, crt, stream);
     if (between) check(cudaEventRecord(between, stream), "cudaEventRecord");
     ReduceParams reduce{};
-    reduce.dots = s.dots + size_t(first) * h.words;
+    reduce.dots = s.dots + size_t(first) * s.dots_stride;
+    reduce.dots_stride = s.dots_stride;
     reduce.out = d_c + size_t(first) * h.limbs;
     reduce.q = s.q;
     reduce.minus_p = s.minus_p;
@@ -153,7 +155,7 @@ WorkLayout work_layout(const negacyclic_plan& s) {
     w.crt_in = at;
     at = align(at + size_t(h.n) * s.padded_r * 4);
     w.dots = at;
-    at = align(at + size_t(h.n) * h.words * 8);
+    at = align(at + size_t(h.n) * s.dots_stride * 8);
     w.result = at;
     at = align(at + size_t(h.n) * h.limbs * 4);
     w.error_flag = at;
@@ -267,6 +269,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
     s.k_convert = 4 * s.padded_limbs;
     s.k_crt = 4 * s.padded_r;
     s.crt_columns = round_up(4 * h.words, 64);
+    s.dots_stride = round_up(h.words, 8);
     try {
         check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&s.copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -733,7 +736,10 @@ int negacyclic_debug_read(negacyclic_plan* s, int which, void* host, size_t* byt
     }
     if (*bytes < size) return fail(NEGACYCLIC_EINVAL, "host buffer too small");
     DeviceGuard guard(s->device);
-    cudaError_t e = cudaMemcpy(host, src, size, cudaMemcpyDeviceToHost);
+    cudaError_t e = which == 2  // word sums: rows of dots_stride words on the device, words returned
+                        ? cudaMemcpy2D(host, size_t(h.words) * 8, src, size_t(s->dots_stride) * 8, size_t(h.words) * 8,
+                                       h.n, cudaMemcpyDeviceToHost)
+                        : cudaMemcpy(host, src, size, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(NEGACYCLIC_ECUDA, cudaGetErrorString(e));
     *bytes = size;
     return NEGACYCLIC_OK;

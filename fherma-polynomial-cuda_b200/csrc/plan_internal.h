@@ -18,6 +18,7 @@ struct negacyclic_plan {
     int device = 0;
     negacyclic::HostPlan host;
     uint32_t r = 0, padded_r = 0, padded_limbs = 0, k_convert = 0, k_crt = 0, crt_columns = 0;
+    uint32_t dots_stride = 0;  // words per row of the CRT word sums: L + 5 rounded up to 8
     uint32_t convert_engine = NEGACYCLIC_GEMM_SIMT, crt_engine = NEGACYCLIC_GEMM_SIMT;
     negacyclic::DevicePrime* primes = nullptr;
     uint2 *fwd = nullptr, *inv = nullptr, *zeta = nullptr;
