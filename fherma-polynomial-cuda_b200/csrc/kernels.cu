@@ -247,7 +247,31 @@ __global__ void __launch_bounds__(512) ntt_inverse_kernel(uint32_t* residues, co
 
 constexpr uint32_t kPerThread = 16;
 
-__device__ __forceinline__ uint32_t padded(uint32_t i) { return i + (i >> 5); }  // bank-conflict padding
+// Shared-memory layout of a length-2^kLog transform: word i is stored at i ^ M(i >> 5), where M
+// XORs column b into the bank bits when bit 5 + b of i is set. The columns were found by an
+// exhaustive check of every warp access of every pass (forward and inverse, 16 values per
+// thread): with them no pass has a bank conflict, where padding one word per 32 left 2-way
+// conflicts in the passes with half-size 2 and 1 or 16. M is linear, and a pass's per-value
+// offsets k t_min share no bits with its group base, so the swizzle of base + k t_min is the
+// swizzle of base (once per group) XOR a compile-time constant.
+template <uint32_t kLog>
+__host__ __device__ constexpr uint32_t swizzle_column(int b) {
+    constexpr uint32_t c8[] = {30, 1, 4};
+    constexpr uint32_t c9[] = {27, 6, 17, 25};
+    constexpr uint32_t c10[] = {27, 13, 8, 26, 8};
+    constexpr uint32_t c11[] = {28, 27, 10, 20, 2, 25};
+    constexpr uint32_t c12[] = {17, 26, 2, 21, 24, 25, 27};
+    constexpr uint32_t c13[] = {27, 6, 17, 25, 11, 6, 15, 2};
+    return kLog == 8 ? c8[b] : kLog == 9 ? c9[b] : kLog == 10 ? c10[b] : kLog == 11 ? c11[b] : kLog == 12 ? c12[b] : c13[b];
+}
+
+template <uint32_t kLog>
+__host__ __device__ constexpr uint32_t swizzle(uint32_t i) {
+    uint32_t m = 0;
+    for (int b = 0; b < int(kLog) - 5; ++b)
+        if ((i >> (5 + b)) & 1u) m ^= swizzle_column<kLog>(b);
+    return i ^ m;
+}
 
 // Cooley-Tukey stages with half-sizes t_min*2^(R-1) .. t_min (forward, merged psi twiddles) on
 // one group of 2^R values. With j = base + k*t_min and base = group_hi * 2^(log t_min + R) + off
@@ -299,7 +323,7 @@ __device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t group_
 }
 
 // One pass of R stages over all of this thread's groups (transform length 2^kLog,
-// 2^(kLog-4) threads). src/dst are shared (padded index) or global (plain index);
+// 2^(kLog-4) threads). src/dst are shared (swizzled index) or global (plain index);
 // kScale multiplies the values stored to global by (f, f_q).
 template <int R, bool kForward, bool kFromGlobal, bool kToGlobal, bool kScale, uint32_t kLogTMin, uint32_t kLog>
 __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, const uint2* __restrict__ table,
@@ -311,6 +335,7 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
         const uint32_t group = threadIdx.x + g * kThreads;
         const uint32_t off = group & ((1u << kLogTMin) - 1);
         const uint32_t base = ((group >> kLogTMin) << (kLogTMin + R)) + off;
+        const uint32_t placed = swizzle<kLog>(base);  // shared-memory place of the group's first word
         // with t_min = 1 a group is 2^R consecutive words (base a multiple of 2^R): global
         // accesses go four words at a time, so a warp instruction covers 16-byte pieces
         constexpr bool kVector = kLogTMin == 0 && R >= 2;
@@ -328,7 +353,7 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
 #pragma unroll
             for (int k = 0; k < (1 << R); ++k) {
                 const uint32_t i = base + (uint32_t(k) << kLogTMin);
-                x[k] = kFromGlobal ? src[i] : src[padded(i)];
+                x[k] = kFromGlobal ? src[i] : src[placed ^ swizzle<kLog>(uint32_t(k) << kLogTMin)];
             }
         }
         if (kForward)
@@ -349,7 +374,7 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
                 if (kToGlobal)
                     dst[i] = x[k];
                 else
-                    dst[padded(i)] = x[k];
+                    dst[placed ^ swizzle<kLog>(uint32_t(k) << kLogTMin)] = x[k];
             }
         }
     }
@@ -694,7 +719,7 @@ template <bool kForward, uint32_t kLog>
 static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const uint2* table, uint32_t r, uint32_t n,
                            uint32_t first, uint32_t count, cudaStream_t stream) {
     constexpr uint32_t kN = 1u << kLog;
-    const size_t smem = (kN + kN / 32) * sizeof(uint32_t);
+    const size_t smem = kN * sizeof(uint32_t);
     auto kernel = kForward ? ntt_forward_blocked_kernel<kLog> : ntt_inverse_blocked_kernel<kLog>;
     static bool configured = false;
     if (!configured) {  // room for several transforms per SM
