@@ -42,9 +42,9 @@ METRIC = "products/s at N=65536,W=1747 (limbs)"
 WORKLOAD = "negacyclic product N=65536, L=1747 limbs (55904-bit random odd q, seed 2), a,b uniform in [0,q)"
 CPU_SAMPLE_N = N // 32  # bounded CPU sample: 2048 coefficients of the same width
 # DRAM bytes (read + write) of one conversion-GEMM launch on this workload, from a one-pass ncu
-# capture (dram__bytes_read.sum 4.33 GB + dram__bytes_write.sum 1.90 GB) of
+# capture (dram__bytes_read.sum 4.32 GB + dram__bytes_write.sum 1.90 GB) of
 #   python bench.py --workload 65536,1747 --steps 1 --warmup 1 --device-only
-CONVERT_DRAM_BYTES = 6.23e9
+CONVERT_DRAM_BYTES = 6.22e9
 
 
 def _load(name, path, package_dir=None):
