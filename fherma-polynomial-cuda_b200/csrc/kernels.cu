@@ -257,11 +257,11 @@ constexpr uint32_t kPerThread = 16;
 template <uint32_t kLog>
 __host__ __device__ constexpr uint32_t swizzle_column(int b) {
     constexpr uint32_t c8[] = {30, 1, 4};
-    constexpr uint32_t c9[] = {27, 6, 17, 25};
+    constexpr uint32_t c9[] = {7, 9, 27, 13};
     constexpr uint32_t c10[] = {27, 13, 8, 26, 8};
-    constexpr uint32_t c11[] = {28, 27, 10, 20, 2, 25};
+    constexpr uint32_t c11[] = {11, 1, 14, 20, 24, 27};
     constexpr uint32_t c12[] = {17, 26, 2, 21, 24, 25, 27};
-    constexpr uint32_t c13[] = {27, 6, 17, 25, 11, 6, 15, 2};
+    constexpr uint32_t c13[] = {7, 9, 27, 13, 8, 26, 8, 13};
     return kLog == 8 ? c8[b] : kLog == 9 ? c9[b] : kLog == 10 ? c10[b] : kLog == 11 ? c11[b] : kLog == 12 ? c12[b] : c13[b];
 }
 
@@ -380,13 +380,16 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
     }
 }
 
-// Passes kDone.. of a length-2^kLog transform: four stages per pass, the remainder last.
-// Forward runs half-sizes large -> small (its short last pass keeps the global stores of
-// consecutive words narrow per thread); inverse small -> large and scales its output.
+// Passes kDone.. of a length-2^kLog transform: four stages per pass, and a shorter pass for the
+// remainder at the unit-stride end, where it touches global memory 2 consecutive words per
+// thread instead of 16: last in the forward transform (half-sizes large -> small), first in the
+// inverse (small -> large, which also scales its output).
 template <bool kForward, uint32_t kLog, uint32_t kDone>
 __device__ __forceinline__ void ntt_passes(uint32_t* data, uint32_t* xs, const uint2* __restrict__ table, uint32_t p,
                                            uint32_t f, uint32_t f_q) {
-    constexpr int R = (kLog - kDone) < 4 ? int(kLog - kDone) : 4;
+    constexpr int R = (!kForward && kDone == 0 && kLog % 4 != 0) ? int(kLog % 4)
+                      : (kLog - kDone) < 4                       ? int(kLog - kDone)
+                                                                  : 4;
     constexpr uint32_t kLogTMin = kForward ? kLog - kDone - R : kDone;
     constexpr bool kFirst = kDone == 0, kLast = kDone + R == kLog;
     ntt_pass<R, kForward, kFirst, kLast, kLast && !kForward, kLogTMin, kLog>(kFirst ? data : xs, kLast ? data : xs,
