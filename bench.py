@@ -10,6 +10,9 @@ per operand: every step reads inputs larger than the 126 MB L2).
             through negacyclic_run_device, CUDA events on the launching stream
   e2e       products/s through negacyclic_run (the host-facing C ABI) with pinned
             host buffers: H2D of a and b and D2H of c inside the timed region
+  batched_e2e  products/s through negacyclic_batch_run: K products (at most 32 GB) of the same
+            workload from page-locked host arrays, copies of one product overlapping
+            the compute of the next (plain_value = e2e, one product per call)
   roofline  the conversion GEMM (the largest kernel): algorithmic int8 ops per
             launch / its CUDA-event time, against the int8 tensor peak
   cpu_baseline  the GMP Kronecker oracle (the reference checker's algorithm) on a
@@ -197,6 +200,36 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def path_roofline(n: int, limbs: int, info: dict, stage_ms: dict, product_ms: float, int8_tops: float,
+                  hbm_gbs: float) -> dict:
+    """Roofline of the whole plain device path: the sum over stages of ops / int8 peak (the two
+    GEMMs) or algorithmic bytes / HBM peak (the rest), against the measured time per product."""
+    r, padded_r, words = info["primes"], info["padded_primes"], info["words"]
+    padded_limbs = (limbs + 31) // 32 * 32
+    dots_stride = (words + 7) // 8 * 8
+    ops = {"convert": 2.0 * (2 * n) * (4 * limbs) * (4 * r), "crt": 2.0 * n * (4 * r) * (4 * words)}
+    hbm_bytes = {
+        "pad": 4.0 * 2 * n * (limbs + padded_limbs),      # read a, b; write padded operand rows
+        "forward": 4.0 * 2 * 2 * r * n,                   # both operands' residues, in place
+        "pointwise": 4.0 * 3 * r * n,                     # read two transform sets, write one
+        "inverse": 4.0 * 2 * r * n,                       # in place
+        "transpose": 4.0 * (r + padded_r) * n,            # prime-major -> coefficient-major
+        "reduce": 8.0 * dots_stride * n + 4.0 * n * limbs,  # word sums in, c out
+    }
+    stages, roof_total = {}, 0.0
+    for name, ms in stage_ms.items():
+        if name in ops:
+            roof, bound, work = ops[name] / (int8_tops * 1e12) * 1e3, "int8 tensor", ops[name]
+        else:
+            roof, bound, work = hbm_bytes[name] / (hbm_gbs * 1e9) * 1e3, "hbm", hbm_bytes[name]
+        roof_total += roof
+        stages[name] = {"ms": round(ms, 4), "roof_ms": round(roof, 4), "bound": bound, "work": work,
+                        "frac": round(roof / ms, 3) if ms > 0 else None}
+    return {"stages": stages, "roof_ms": round(roof_total, 3), "measured_ms": round(product_ms, 3),
+            "measured_over_roof": round(product_ms / roof_total, 3),
+            "peaks": {"int8_tops": int8_tops, "hbm_gbs": hbm_gbs}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -271,6 +304,31 @@ def run_b200(args):
     if not np.array_equal(dc.cpu().numpy().view(np.uint32), hc):
         raise RuntimeError("device-resident and host products differ")
 
+    # --- batched form on the same workload: K products from the same page-locked host arrays
+    # through negacyclic_batch_run (copy-in, compute and copy-out streams overlap across products)
+    batched = None
+    if not args.no_batched:
+        count = max(4, min(args.steps, int(32e9 // (3 * a.nbytes))))  # device slots: at most 32 GB
+        t1 = time.perf_counter()
+        batch = fpc.Batch([(n_coeff, 32 * limbs, limbs, q)] * count, device=local)
+        setup_s = time.perf_counter() - t1
+        pcb = torch.empty_like(pa).pin_memory()
+        hcb = pcb.numpy().view(np.uint32)
+        batch.run([ha] * count, [hb] * count, [hcb] * count)  # warm-up
+        batch_s = []
+        for _ in range(2):
+            barrier()
+            t1 = time.perf_counter()
+            batch.run([ha] * count, [hb] * count, [hcb] * count)
+            batch_s.append(max_over_ranks(time.perf_counter() - t1, world, "cuda"))
+        batch.close()
+        if not np.array_equal(hcb, hc):
+            raise RuntimeError("batched and per-call products differ")
+        batched = {"value": replica_throughput(world, count, min(batch_s)), "unit": "products/s",
+                   "products_per_call": count, "api": "negacyclic_batch_run, page-locked host arrays",
+                   "h2d_bytes_per_product": int(a.nbytes + b.nbytes), "d2h_bytes_per_product": int(a.nbytes),
+                   "plain_value": e2e_value, "setup_s": round(setup_s, 2)}
+
     # --- roofline of the conversion GEMM: 2 ops per byte MAC, M=2N rows, K=4L bytes, 4r weight columns
     hbm_gbs, bf16_tflops, source = peaks()
     int8_peak = 2 * bf16_tflops  # dense int8 = 2x dense bf16 on B200 (4.5 vs 2.25 PFLOP/s nominal)
@@ -291,6 +349,7 @@ def run_b200(args):
         "algorithmic_ops_per_launch": conv_ops,
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "crt_gemm_tops": round(crt_ops / (stage_ms["crt"] / 1000) / 1e12, 1),
+        "whole_path": path_roofline(n_coeff, limbs, info, stage_ms, device_ms / args.steps, int8_peak, hbm_gbs),
     }
 
     cpu = None
@@ -312,6 +371,7 @@ def run_b200(args):
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "products/s", "h2d_bytes_per_step": int(a.nbytes + b.nbytes),
                     "d2h_bytes_per_step": int(a.nbytes)},
+            "batched_e2e": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
@@ -525,6 +585,7 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    parser.add_argument("--no-batched", action="store_true", help="skip the batched host-array measurement")
     parser.add_argument("--workload", default=f"{N},{LIMBS}",
                         help="N,L of a smaller case for profiling (the benchmark line is N=65536,L=1747)")
     parser.add_argument("--device-only", action="store_true",

@@ -278,6 +278,9 @@ __host__ __device__ constexpr uint32_t swizzle(uint32_t i) {
 // (off < t_min), butterfly (k, k + half) of stage r has twiddle m + (j >> (log t + 1))
 // = m + group_hi * 2^r + (k >> (R - r)): the 2^(R-1-r) butterflies of block b = k >> (R - r)
 // share one twiddle, so a pass loads 2^R - 1 twiddles for its R * 2^(R-1) butterflies.
+// Values between stages are kept in [0, 2p) (2p < 2^32): each butterfly reduces its two inputs
+// once, so that u + v and u - v + p stay below 2p, and multiplies by the twiddle without
+// Shoup's final correction. Canonical inputs are a special case; the last pass reduces.
 template <int R>
 __device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t group_hi, uint32_t log_t_min,
                                           uint32_t log_n, const uint2* __restrict__ table, uint32_t p) {
@@ -291,9 +294,10 @@ __device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t group_
             const uint2 w = __ldg(&table[m + (group_hi << r) + b]);
 #pragma unroll
             for (int k = b * 2 * half; k < b * 2 * half + half; ++k) {
-                const uint32_t u = x[k], v = shoup(x[k + half], w.x, w.y, p);
-                x[k] = add_mod(u, v, p);
-                x[k + half] = sub_mod(u, v, p);
+                const uint32_t u = reduce_once(x[k], p);
+                const uint32_t v = reduce_once(shoup_lazy(x[k + half], w.x, w.y, p), p);
+                x[k] = u + v;
+                x[k + half] = u - v + p;
             }
         }
     }
@@ -301,6 +305,7 @@ __device__ __forceinline__ void ct_stages(uint32_t (&x)[1 << R], uint32_t group_
 
 // Gentleman-Sande stages with half-sizes t_min .. t_min*2^(R-1) (inverse). Stage r's butterflies
 // (k, k + 2^r) in block b = k >> (r + 1) share twiddle h + group_hi * 2^(R-1-r) + b.
+// Values between stages are in [0, 2p), as in ct_stages.
 template <int R>
 __device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t group_hi, uint32_t log_t_min,
                                           uint32_t log_n, const uint2* __restrict__ table, uint32_t p) {
@@ -314,9 +319,9 @@ __device__ __forceinline__ void gs_stages(uint32_t (&x)[1 << R], uint32_t group_
             const uint2 w = __ldg(&table[h + (group_hi << (R - 1 - r)) + b]);
 #pragma unroll
             for (int k = b * 2 * half; k < b * 2 * half + half; ++k) {
-                const uint32_t u = x[k], v = x[k + half];
-                x[k] = add_mod(u, v, p);
-                x[k + half] = shoup(sub_mod(u, v, p), w.x, w.y, p);
+                const uint32_t u = reduce_once(x[k], p), v = reduce_once(x[k + half], p);
+                x[k] = u + v;
+                x[k + half] = shoup_lazy(u - v + p, w.x, w.y, p);
             }
         }
     }
@@ -361,8 +366,12 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
         else
             gs_stages<R>(x, group >> kLogTMin, kLogTMin, kLog, table, p);
 #pragma unroll
-        for (int k = 0; k < (1 << R); ++k)
-            if (kScale) x[k] = shoup(x[k], f, f_q, p);
+        for (int k = 0; k < (1 << R); ++k) {
+            if (kScale)
+                x[k] = shoup(x[k], f, f_q, p);  // canonical: shoup takes any 32-bit value
+            else if (kToGlobal)
+                x[k] = reduce_once(x[k], p);    // [0, 2p) -> canonical
+        }
         if constexpr (kToGlobal && kVector) {
 #pragma unroll
             for (int q = 0; q < (1 << R) / 4; ++q)

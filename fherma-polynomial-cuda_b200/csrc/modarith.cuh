@@ -60,6 +60,13 @@ __device__ __forceinline__ uint32_t pow_mod(uint32_t base, uint64_t e, const Dev
     return mont(acc, 1, f.p, f.pinv);
 }
 
+// shoup without its final correction: a w mod p + {0 or p}, in [0, 2p) for any 32-bit a
+// (the quotient estimate is at most one short; Harvey, "Faster arithmetic for number-theoretic
+// transforms", J. Symb. Comput. 60 (2014), lemma on Shoup's multiplication)
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t a, uint32_t w, uint32_t w_q, uint32_t p) {
+    return a * w - __umulhi(a, w_q) * p;
+}
+
 __device__ __forceinline__ uint32_t shoup_quotient(uint32_t w, uint32_t p) {
     return uint32_t((uint64_t(w) << 32) / p);
 }
