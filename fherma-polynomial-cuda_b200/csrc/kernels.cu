@@ -12,6 +12,7 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace negacyclic {
 
@@ -435,64 +436,100 @@ __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_in
 }
 
 // C_v = sum_{t+u=v} A_t B_u + zeta * sum_{t+u=v+s} A_t B_u at every evaluation point,
-// written over A_v. Products are Montgomery (x y 2^-32).
-template <int S>
+// written over A_v. Products are Montgomery (x y 2^-32). Each thread takes V consecutive
+// evaluation points (V = 2: 8-byte accesses, n_sub even).
+template <int S, int V>
 __global__ void pointwise_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
                                  const uint2* __restrict__ zeta, uint32_t r, uint32_t n, uint32_t n_sub) {
+    using Word = std::conditional_t<V == 2, uint2, uint32_t>;
     const uint32_t k = blockIdx.y;
-    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) * V;
     if (m >= n_sub) return;
     const DevicePrime f = primes[k];
-    uint32_t* a = residues + size_t(k) * n + m;
-    const uint32_t* b = residues + (size_t(r) + k) * n + m;
-    uint32_t av[S], bv[S];
+    Word* a = reinterpret_cast<Word*>(residues + size_t(k) * n + m);
+    const Word* b = reinterpret_cast<const Word*>(residues + (size_t(r) + k) * n + m);
+    const size_t step = n_sub / V;  // one transform, in Words
+    uint32_t av[V][S], bv[V][S];
 #pragma unroll
     for (int t = 0; t < S; ++t) {
-        av[t] = a[size_t(t) * n_sub];
-        bv[t] = b[size_t(t) * n_sub];
+        const Word x = a[t * step], y = b[t * step];
+        if constexpr (V == 2) {
+            av[0][t] = x.x, av[1][t] = x.y, bv[0][t] = y.x, bv[1][t] = y.y;
+        } else {
+            av[0][t] = x, bv[0][t] = y;
+        }
     }
-    const uint2 z = zeta[size_t(k) * n_sub + m];
+    uint2 z[V];
+    if constexpr (V == 2) {
+        const uint4 zz = *reinterpret_cast<const uint4*>(zeta + size_t(k) * n_sub + m);
+        z[0] = make_uint2(zz.x, zz.y), z[1] = make_uint2(zz.z, zz.w);
+    } else {
+        z[0] = zeta[size_t(k) * n_sub + m];
+    }
     // two products per Montgomery reduction: a b + a' b' < 2 p^2 < p 2^32
 #pragma unroll
     for (int v = 0; v < S; ++v) {
-        uint32_t low = 0, wrap = 0;
+        uint32_t out[V];
 #pragma unroll
-        for (int t = 0; t <= v; t += 2) {
-            uint64_t pair = uint64_t(av[t]) * bv[v - t];
-            if (t + 1 <= v) pair += uint64_t(av[t + 1]) * bv[v - t - 1];
-            low = add_mod(low, redc(pair, f.p, f.pinv), f.p);
-        }
+        for (int e = 0; e < V; ++e) {
+            uint32_t low = 0, wrap = 0;
 #pragma unroll
-        for (int t = v + 1; t < S; t += 2) {
-            uint64_t pair = uint64_t(av[t]) * bv[v + S - t];
-            if (t + 1 < S) pair += uint64_t(av[t + 1]) * bv[v + S - t - 1];
-            wrap = add_mod(wrap, redc(pair, f.p, f.pinv), f.p);
+            for (int t = 0; t <= v; t += 2) {
+                uint64_t pair = uint64_t(av[e][t]) * bv[e][v - t];
+                if (t + 1 <= v) pair += uint64_t(av[e][t + 1]) * bv[e][v - t - 1];
+                low = add_mod(low, redc(pair, f.p, f.pinv), f.p);
+            }
+#pragma unroll
+            for (int t = v + 1; t < S; t += 2) {
+                uint64_t pair = uint64_t(av[e][t]) * bv[e][v + S - t];
+                if (t + 1 < S) pair += uint64_t(av[e][t + 1]) * bv[e][v + S - t - 1];
+                wrap = add_mod(wrap, redc(pair, f.p, f.pinv), f.p);
+            }
+            out[e] = add_mod(low, shoup(wrap, z[e].x, z[e].y, f.p), f.p);
         }
-        a[size_t(v) * n_sub] = add_mod(low, shoup(wrap, z.x, z.y, f.p), f.p);
+        if constexpr (V == 2)
+            a[v * step] = make_uint2(out[0], out[1]);
+        else
+            a[v * step] = out[0];
     }
 }
 
 // residues[0][k][v*N' + j] -> crt_in[s*j + v][k] (coefficient-major) for every transform v and
 // j in [j_first, j_first + j_count), i.e. coefficients [s j_first, s (j_first + j_count)); zero for
-// k in [r, r'). Block x covers up to 32 consecutive j of one transform.
-__global__ void transpose_kernel(const uint32_t* __restrict__ residues, uint32_t* __restrict__ crt_in,
-                                 uint32_t r, uint32_t padded_r, uint32_t n, uint32_t log_split, uint32_t log_n_sub,
-                                 uint32_t j_first, uint32_t j_count) {
-    __shared__ uint32_t tile[32][33];
-    const uint32_t blocks_per_v = (j_count + 31) / 32, v = blockIdx.x / blocks_per_v;
-    const uint32_t j0 = j_first + (blockIdx.x - v * blocks_per_v) * 32, k0 = blockIdx.y * 32;
+// k in [r, r'). Block x covers up to 64 consecutive j of one transform and block y 64 primes, so
+// every global access is a 256-byte run (two warp instructions of 128 bytes); the tile's rows are
+// padded to 65 words, which keeps both the row-wise writes and the column-wise reads free of bank
+// conflicts. 256 threads: 16 loads in flight per thread.
+constexpr uint32_t kTransposeTile = 64;
+__global__ void __launch_bounds__(256) transpose_kernel(const uint32_t* __restrict__ residues,
+                                                        uint32_t* __restrict__ crt_in, uint32_t r, uint32_t padded_r,
+                                                        uint32_t n, uint32_t log_split, uint32_t log_n_sub,
+                                                        uint32_t j_first, uint32_t j_count) {
+    __shared__ uint32_t tile[kTransposeTile][kTransposeTile + 1];
+    const uint32_t blocks_per_v = (j_count + kTransposeTile - 1) / kTransposeTile, v = blockIdx.x / blocks_per_v;
+    const uint32_t j0 = j_first + (blockIdx.x - v * blocks_per_v) * kTransposeTile, k0 = blockIdx.y * kTransposeTile;
     const uint32_t j_end = j_first + j_count, rho0 = (v << log_n_sub) + j0;
-    const uint32_t x = threadIdx.x, y = threadIdx.y;
-    for (uint32_t dy = 0; dy < 32; dy += 8) {
-        uint32_t k = k0 + y + dy;
-        tile[y + dy][x] = (k < r && j0 + x < j_end) ? residues[size_t(k) * n + rho0 + x] : 0u;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 8 warps
+#pragma unroll
+    for (uint32_t row = warp; row < kTransposeTile; row += 8) {  // row = prime offset
+        const uint32_t k = k0 + row;
+#pragma unroll
+        for (uint32_t half = 0; half < kTransposeTile; half += 32) {
+            const uint32_t j = j0 + half + lane;
+            tile[row][half + lane] = (k < r && j < j_end) ? residues[size_t(k) * n + rho0 + half + lane] : 0u;
+        }
     }
     __syncthreads();
-    for (uint32_t dy = 0; dy < 32; dy += 8) {
-        uint32_t j = j0 + y + dy, k = k0 + x;
-        if (k >= padded_r || j >= j_end) continue;
-        const size_t coefficient = (size_t(j) << log_split) + v;
-        crt_in[coefficient * padded_r + k] = tile[x][y + dy];
+#pragma unroll
+    for (uint32_t row = warp; row < kTransposeTile; row += 8) {  // row = position offset
+        const uint32_t j = j0 + row;
+        if (j >= j_end) continue;
+        uint32_t* out = crt_in + ((size_t(j) << log_split) + v) * padded_r;
+#pragma unroll
+        for (uint32_t half = 0; half < kTransposeTile; half += 32) {
+            const uint32_t k = k0 + half + lane;
+            if (k < padded_r) out[k] = tile[half + lane][row];
+        }
     }
 }
 
@@ -774,22 +811,33 @@ void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uin
 
 void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r, uint32_t n,
                       uint32_t n_sub, uint32_t split, cudaStream_t stream) {
+    if (n_sub % 2 == 0) {  // two evaluation points per thread
+        dim3 grid((n_sub / 2 + 127) / 128, r);
+        switch (split) {
+            case 1: pointwise_kernel<1, 2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+            case 2: pointwise_kernel<2, 2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+            case 4: pointwise_kernel<4, 2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+            case 8: pointwise_kernel<8, 2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+            default: pointwise_kernel<16, 2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        }
+        return;
+    }
     dim3 grid((n_sub + 127) / 128, r);
     switch (split) {
-        case 1: pointwise_kernel<1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
-        case 2: pointwise_kernel<2><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
-        case 4: pointwise_kernel<4><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
-        case 8: pointwise_kernel<8><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
-        default: pointwise_kernel<16><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 1: pointwise_kernel<1, 1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 2: pointwise_kernel<2, 1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 4: pointwise_kernel<4, 1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        case 8: pointwise_kernel<8, 1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
+        default: pointwise_kernel<16, 1><<<grid, 128, 0, stream>>>(residues, primes, zeta, r, n, n_sub); break;
     }
 }
 
 void launch_transpose(const uint32_t* residues, uint32_t* crt_in, uint32_t r, uint32_t padded_r, uint32_t n,
                       uint32_t split, uint32_t j_first, uint32_t j_count, cudaStream_t stream) {
     const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
-    dim3 grid(split * ((j_count + 31) / 32), padded_r / 32);
-    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(residues, crt_in, r, padded_r, n, log_split, log_n_sub,
-                                                       j_first, j_count);
+    dim3 grid(split * ((j_count + kTransposeTile - 1) / kTransposeTile), (padded_r + kTransposeTile - 1) / kTransposeTile);
+    transpose_kernel<<<grid, 256, 0, stream>>>(residues, crt_in, r, padded_r, n, log_split, log_n_sub, j_first,
+                                               j_count);
 }
 
 void launch_reduce(const ReduceParams& params, cudaStream_t stream) {
