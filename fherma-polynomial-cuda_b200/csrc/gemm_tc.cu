@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
 //     CTAs at once (tcgen05.commit ... multicast::cluster, mask 0b11);
 //   * all eight epilogue warps of the pair release an accumulator on the
 //     leader's acc_empty[a] (cluster-scope arrive).
-constexpr uint32_t kPairStages = 6;
+constexpr uint32_t kPairStages = 7;  // 224 KB of ring: seven stages fit the 227 KB opt-in limit with the barriers
 constexpr uint32_t kPairBlockN = 256;                      // columns per pair tile
 constexpr uint32_t kPairBTileBytes = (kPairBlockN / 2) * kBlockK;  // 16 KB: this CTA's half of B
 constexpr uint32_t kPairStageBytes = kATileBytes + kPairBTileBytes; // 32 KB per CTA
