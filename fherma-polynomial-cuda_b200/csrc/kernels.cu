@@ -630,34 +630,48 @@ __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
         const uint64_t low = x0 + (x1 << 32);
         const uint64_t high = (x1 >> 32) + x2 + (low < x0 ? 1 : 0);  // D = high 2^64 + low
         const uint64_t kq = high + ((low + (1ull << 63)) < low ? 1 : 0);
-        // 2. T' = sum_w (d[w] + K R[w]) 2^(32w), collapsed to exact words in one carry pass.
-        //    The word sums come from DRAM: kBatch steps' worth are loaded before any is used, so
-        //    one load latency covers kBatch 32-word steps of the (serial) carry chain.
-        constexpr uint32_t kBatch = 8;
+        // 2. T' = sum_w (d[w] + K R[w]) 2^(32w), collapsed to exact words in one carry pass. A lane
+        //    holds words w0 = base + 2 lane and w0 + 1 of a 64-word step: its two word sums meet
+        //    in-lane, the bits at 2^64 and up go to the next lane by a shuffle (< 2^25), and one
+        //    warp-wide carry resolution covers 64 words. The word sums come from DRAM in 16-byte
+        //    pairs, kBatch steps' worth before any is used, so one load latency covers kBatch steps
+        //    of the (serial) carry chain. K < 2r fits 32 bits.
+        constexpr uint32_t kBatch = 4;
+        const uint32_t k32 = uint32_t(kq);
         uint32_t chain = 0, carried_high = 0;
-        for (uint32_t batch = 0; batch < tlen; batch += 32 * kBatch) {
-            uint64_t loaded[kBatch];
-            uint32_t r_words[kBatch];
+        for (uint32_t batch = 0; batch < tlen; batch += 64 * kBatch) {
+            uint64_t x0[kBatch], x1[kBatch];
 #pragma unroll
             for (uint32_t u = 0; u < kBatch; ++u) {
-                const uint32_t w = batch + 32 * u + lane;
-                loaded[u] = w < tlen ? d[w] : 0ull;
-                r_words[u] = w < limbs ? prm.minus_p[w] : 0u;
+                const uint32_t w0 = batch + 64 * u + 2 * lane;
+                uint64_t d0 = 0, d1 = 0;
+                if (w0 < tlen) {  // w0 + 1 < dots_stride: the row holds at least tlen + 3 words
+                    const ulonglong2 pair = *reinterpret_cast<const ulonglong2*>(d + w0);
+                    d0 = pair.x;
+                    d1 = w0 + 1 < tlen ? pair.y : 0ull;
+                }
+                const uint32_t r0 = w0 < limbs ? prm.minus_p[w0] : 0u, r1 = w0 + 1 < limbs ? prm.minus_p[w0 + 1] : 0u;
+                x0[u] = d0 + uint64_t(k32) * r0;  // < 2^57
+                x1[u] = d1 + uint64_t(k32) * r1;
             }
 #pragma unroll
             for (uint32_t u = 0; u < kBatch; ++u) {
-                const uint32_t base = batch + 32 * u;
+                const uint32_t base = batch + 64 * u;
                 if (base >= tlen) break;  // warp-uniform
-                const uint32_t w = base + lane;
-                const uint64_t value = loaded[u] + kq * r_words[u];  // both zero past the end
-                const uint32_t high32 = uint32_t(value >> 32);
-                uint32_t below = __shfl_up_sync(kFull, high32, 1);
+                const uint32_t w0 = base + 2 * lane;
+                const uint32_t top = uint32_t(x1[u] >> 32);
+                uint32_t below = __shfl_up_sync(kFull, top, 1);
                 if (lane == 0) below = carried_high;
-                carried_high = __shfl_sync(kFull, high32, 31);
-                const uint64_t sum = uint64_t(uint32_t(value)) + below;
-                const uint32_t word = uint32_t(sum);
-                const uint32_t carry = chain_carry((sum >> 32) != 0, word == kFull, chain);
-                if (w < tlen) v[w] = word + carry;
+                carried_high = __shfl_sync(kFull, top, 31);
+                const uint64_t s0 = uint64_t(uint32_t(x0[u])) + below;                     // < 2^33
+                const uint64_t s1 = (x0[u] >> 32) + uint32_t(x1[u]) + uint32_t(s0 >> 32);  // < 2^33
+                uint32_t word0 = uint32_t(s0), word1 = uint32_t(s1);
+                const bool generate = (s1 >> 32) != 0;
+                const uint32_t carry = chain_carry(generate, !generate && (word0 & word1) == kFull, chain);
+                word0 += carry;
+                word1 += (carry != 0 && word0 == 0) ? 1u : 0u;
+                if (w0 < tlen) v[w0] = word0;
+                if (w0 + 1 < tlen) v[w0 + 1] = word1;
             }
         }
         __syncwarp();
@@ -673,30 +687,40 @@ __global__ void reduce_kernel(ReduceParams prm, uint32_t stride) {
         const uint64_t quotient = th + word2 + ((tl + word1 < tl) ? 1 : 0);
         const uint32_t ql = uint32_t(quotient), qh = uint32_t(quotient >> 32);
         __syncwarp();
-        // 4. c = T' - quotient*q in one signed carry pass. With a_w = ql q[w], b_w = qh q[w-1]:
-        //    z_w = T'[w] - lo(a_w) - lo(b_w) - hi(a_{w-1}) - hi(b_{w-1})  in (-2^35, 2^32)
+        // 4. c = T' - quotient*q in one signed carry pass, two words per lane as in step 2. With
+        //    a_w = ql q[w], b_w = qh q[w-1]:
+        //    z_w = T'[w] - lo(a_w) - lo(b_w) - hi(a_{w-1}) - hi(b_{w-1})  in (-2^35, 2^32),
+        //    c_w = floor(z_w / 2^32) in [-8, 0] moves to word w + 1, leaving sw_w in [-8, 2^32) and a
+        //    one-bit borrow chain. A lane generates a borrow when sw1 < 0, or sw1 = 0 and sw0 < 0,
+        //    and passes one on when sw1 = sw0 = 0.
         chain = 0;
-        uint64_t carry_hi = 0;  // hi(a)+hi(b) of the previous chunk's last lane
-        int32_t carry_c = 0;    // signed word carry of the previous chunk's last lane
-        for (uint32_t base = 0; base < tlen; base += 32) {
-            const uint32_t w = base + lane;
-            const uint32_t qw = w < limbs ? q[w] : 0u;
-            const uint32_t qw1 = (w >= 1 && w - 1 < limbs) ? q[w - 1] : 0u;
-            const uint64_t a = uint64_t(ql) * qw, b = uint64_t(qh) * qw1;
-            const uint64_t hi = (a >> 32) + (b >> 32);
-            uint64_t hi_below = (uint64_t(__shfl_up_sync(kFull, uint32_t(hi >> 32), 1)) << 32) |
-                                __shfl_up_sync(kFull, uint32_t(hi), 1);
+        uint64_t carry_hi = 0;  // hi(a)+hi(b) of the previous step's last word
+        int32_t carry_c = 0;    // signed word carry of the previous step's last word
+        for (uint32_t base = 0; base < tlen; base += 64) {
+            const uint32_t w0 = base + 2 * lane, w1 = w0 + 1;
+            const uint32_t qa = w0 < limbs ? q[w0] : 0u, qb = w1 < limbs ? q[w1] : 0u;
+            const uint32_t qm = (w0 >= 1 && w0 - 1 < limbs) ? q[w0 - 1] : 0u;
+            const uint64_t a0 = uint64_t(ql) * qa, b0 = uint64_t(qh) * qm;  // word w0
+            const uint64_t a1 = uint64_t(ql) * qb, b1 = uint64_t(qh) * qa;  // word w1
+            const uint64_t hi0 = (a0 >> 32) + (b0 >> 32), hi1 = (a1 >> 32) + (b1 >> 32);
+            uint64_t hi_below = (uint64_t(__shfl_up_sync(kFull, uint32_t(hi1 >> 32), 1)) << 32) |
+                                __shfl_up_sync(kFull, uint32_t(hi1), 1);
             if (lane == 0) hi_below = carry_hi;
-            carry_hi = (uint64_t(__shfl_sync(kFull, uint32_t(hi >> 32), 31)) << 32) | __shfl_sync(kFull, uint32_t(hi), 31);
-            const uint64_t e = (a & 0xffffffffull) + (b & 0xffffffffull) + hi_below;
-            const int64_t z = int64_t(w < tlen ? v[w] : 0u) - int64_t(e);
-            const int32_t c = int32_t(z >> 32);  // floor(z / 2^32), in [-8, 0]
-            int32_t c_below = __shfl_up_sync(kFull, c, 1);
+            carry_hi = (uint64_t(__shfl_sync(kFull, uint32_t(hi1 >> 32), 31)) << 32) | __shfl_sync(kFull, uint32_t(hi1), 31);
+            const uint64_t e0 = (a0 & 0xffffffffull) + (b0 & 0xffffffffull) + hi_below;
+            const uint64_t e1 = (a1 & 0xffffffffull) + (b1 & 0xffffffffull) + hi0;
+            const int64_t z0 = int64_t(w0 < tlen ? v[w0] : 0u) - int64_t(e0);
+            const int64_t z1 = int64_t(w1 < tlen ? v[w1] : 0u) - int64_t(e1);
+            const int32_t c0 = int32_t(z0 >> 32), c1 = int32_t(z1 >> 32);
+            int32_t c_below = __shfl_up_sync(kFull, c1, 1);
             if (lane == 0) c_below = carry_c;
-            carry_c = __shfl_sync(kFull, c, 31);
-            const int64_t sw = int64_t(uint32_t(z)) + c_below;  // in [-8, 2^32)
-            const uint32_t borrow = chain_carry(sw < 0, sw == 0, chain);
-            if (w < tlen) v[w] = uint32_t(sw - borrow);
+            carry_c = __shfl_sync(kFull, c1, 31);
+            const int64_t sw0 = int64_t(uint32_t(z0)) + c_below, sw1 = int64_t(uint32_t(z1)) + c0;
+            const bool generate = sw1 < 0 || (sw1 == 0 && sw0 < 0);
+            const uint32_t borrow = chain_carry(generate, !generate && sw1 == 0 && sw0 == 0, chain);
+            const int64_t t0 = sw0 - borrow;
+            if (w0 < tlen) v[w0] = uint32_t(t0);
+            if (w1 < tlen) v[w1] = uint32_t(sw1 - (t0 < 0 ? 1 : 0));
         }
         __syncwarp();
         // 5. at most three subtractions of q remain
