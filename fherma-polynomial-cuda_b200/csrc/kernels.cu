@@ -343,10 +343,16 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
         const uint32_t base = ((group >> kLogTMin) << (kLogTMin + R)) + off;
         const uint32_t placed = swizzle<kLog>(base);  // shared-memory place of the group's first word
         // with t_min = 1 a group is 2^R consecutive words (base a multiple of 2^R): global
-        // accesses go four words at a time, so a warp instruction covers 16-byte pieces
+        // accesses go four words at a time (two in a one-stage pass), so a warp instruction
+        // covers 16-byte (8-byte) pieces
         constexpr bool kVector = kLogTMin == 0 && R >= 2;
+        constexpr bool kPair = kLogTMin == 0 && R == 1;
         uint32_t x[1 << R];
-        if constexpr (kFromGlobal && kVector) {
+        if constexpr (kFromGlobal && kPair) {
+            const uint2 w = *reinterpret_cast<const uint2*>(src + base);
+            x[0] = w.x;
+            x[1] = w.y;
+        } else if constexpr (kFromGlobal && kVector) {
 #pragma unroll
             for (int q = 0; q < (1 << R) / 4; ++q) {
                 const uint4 w = reinterpret_cast<const uint4*>(src + base)[q];
@@ -373,7 +379,9 @@ __device__ __forceinline__ void ntt_pass(const uint32_t* src, uint32_t* dst, con
             else if (kToGlobal)
                 x[k] = reduce_once(x[k], p);    // [0, 2p) -> canonical
         }
-        if constexpr (kToGlobal && kVector) {
+        if constexpr (kToGlobal && kPair) {
+            *reinterpret_cast<uint2*>(dst + base) = make_uint2(x[0], x[1]);
+        } else if constexpr (kToGlobal && kVector) {
 #pragma unroll
             for (int q = 0; q < (1 << R) / 4; ++q)
                 reinterpret_cast<uint4*>(dst + base)[q] = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
