@@ -294,7 +294,10 @@ typedef struct {
 int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_server** server);
 
 /* Opens a session for (W, L, q); plans for the `count` ring sizes in ns are built now
- * (others on their first request). */
+ * (others on their first request). The first request that launches a given kernel instance
+ * (for instance the first of a new ring size) also loads that kernel's module, which costs tens
+ * of milliseconds. A latency-sensitive caller sends one request per (session, N) before serving,
+ * or sets CUDA_MODULE_LOADING=EAGER to load every module when the library is first used. */
 int negacyclic_server_open_session(negacyclic_server* server, uint32_t w, uint32_t limbs,
                                    const uint32_t* q, const uint32_t* ns, uint32_t count,
                                    uint32_t* session);
