@@ -79,3 +79,22 @@ def test_single_process_needs_no_process_group():
     bench = _bench()
     assert bench.max_over_ranks(3.5, 1) == 3.5
     assert bench.replica_throughput(1, 20, 0.5) == 40.0
+
+
+def test_whole_path_roofline_arithmetic():
+    """bench.py's per-stage roofline: GEMM stages against the int8 figure, the rest against HBM,
+    summed and set against the measured time per product (N=65536, L=1747, r=3636)."""
+    bench = _bench()
+    info = {"primes": 3636, "padded_primes": 3648, "words": 1752}
+    stage_ms = {"pad": 0.31, "convert": 8.8, "forward": 2.0, "pointwise": 0.67, "inverse": 1.2,
+                "transpose": 0.3, "crt": 4.4, "reduce": 0.6}
+    out = bench.path_roofline(65536, 1747, info, stage_ms, 18.6, 2766.0, 6549.4)
+    stages = out["stages"]
+    assert stages["convert"]["bound"] == "int8 tensor" and stages["reduce"]["bound"] == "hbm"
+    assert stages["convert"]["work"] == 2.0 * (2 * 65536) * (4 * 1747) * (4 * 3636)
+    assert stages["forward"]["work"] == 4.0 * 2 * 2 * 3636 * 65536
+    assert stages["convert"]["roof_ms"] == pytest.approx(stages["convert"]["work"] / 2766e12 * 1e3, abs=1e-4)
+    assert stages["pointwise"]["roof_ms"] == pytest.approx(4.0 * 3 * 3636 * 65536 / 6549.4e9 * 1e3, abs=1e-4)
+    assert out["roof_ms"] == pytest.approx(sum(s["roof_ms"] for s in stages.values()), abs=1e-2)
+    assert out["measured_over_roof"] == pytest.approx(18.6 / out["roof_ms"], rel=1e-2)
+    assert 16.0 < out["roof_ms"] < 17.0  # 14.4 ms of GEMMs + 2.1 ms of HBM stages
