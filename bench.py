@@ -13,13 +13,29 @@ per operand: every step reads inputs larger than the 126 MB L2).
   batched_e2e  products/s through negacyclic_batch_run: K products (at most 32 GB) of the same
             workload from page-locked host arrays, copies of one product overlapping
             the compute of the next (plain_value = e2e, one product per call)
+  e2e_fherma_run  the same metric through fherma_run exactly as the platform harness
+            calls it: pageable std::vectors in and a freshly allocated output vector
+            (fherma-polynomial-cuda_b200/fherma_timer, steady_clock around each call)
+  config2   N=32768, L=868 (q from seed 1): 20 seeded instances, device-resident and
+            end to end (page-locked host buffers)
   roofline  the conversion GEMM (the largest kernel): algorithmic int8 ops per
-            launch / its CUDA-event time, against the int8 tensor peak
+            launch / its CUDA-event time, against the int8 tensor peak (2 x the
+            measured burst bf16 figure; the sustained figure beside it)
+  refpoints the reference's own points (N=65536, W=1747 bits; N=32768, W=868 bits;
+            the checker's prime q and its 20 stress seeds): per-case fherma_run medians
+            of the reference's best entries (candidates/ordered-streaming,
+            candidates/caller-fused-strips, built for sm_100a) and of this library
+            behind the same unmodified harness, all outputs checked against the
+            reference checker's hashes
   cpu_baseline  the GMP Kronecker oracle (the reference checker's algorithm) on a
-            bounded sample (N/32 coefficients, same q width), scaled to one product
+            bounded sample (N/16 coefficients, same q width), scaled to one product by
+            the full-size/sample time ratio measured once on the GPU box's host
+            (--mode cpu-calibrate)
 
-Multi-GPU (torchrun): one independent product stream per GPU (replicas, weak
-scaling), barrier + synchronize around the timed region, max time over ranks.
+Multi-GPU: one independent product stream per GPU (replicas, weak scaling),
+barrier + synchronize around the timed region, max time over ranks. Under
+torchrun the ranks come from its environment; `--gpus N` without it relaunches
+this script under torch.distributed.run with N ranks.
 --impl reference times the reference's CPU path (the oracle port, all host
 cores, one independent sample per core) on the same workload.
 """
@@ -43,11 +59,16 @@ PACKAGE_DIR = os.path.join(REPO, "fherma-polynomial-cuda_b200")
 N, LIMBS, SEED = 65536, 1747, 2
 METRIC = "products/s at N=65536,W=1747 (limbs)"
 WORKLOAD = "negacyclic product N=65536, L=1747 limbs (55904-bit random odd q, seed 2), a,b uniform in [0,q)"
-CPU_SAMPLE_N = N // 32  # bounded CPU sample: 2048 coefficients of the same width
+CPU_SAMPLE_N = N // 16  # bounded CPU sample: 4096 coefficients of the same width
+# GMP's product is superlinear: one full N=65536, L=1747 Kronecker product against the N=4096
+# sample, timed back to back on one core of the GPU box's host (bench.py --mode cpu-calibrate;
+# profiles/cpu_baseline_gmp_N65536_L1747.md); without it the linear factor N / CPU_SAMPLE_N is used
+CPU_FULL_OVER_SAMPLE = 19.35  # 77.74 s against 4.01 s (median of 3), 16-core Xeon host of a B200 box
 # DRAM bytes (read + write) of one conversion-GEMM launch on this workload, from a one-pass ncu
 # capture (dram__bytes_read.sum 4.32 GB + dram__bytes_write.sum 1.90 GB) of
 #   python bench.py --workload 65536,1747 --steps 1 --warmup 1 --device-only
 CONVERT_DRAM_BYTES = 6.22e9
+CONVERT_TENSOR_PIPE_ACTIVE = 0.833
 
 
 def _load(name, path, package_dir=None):
@@ -66,14 +87,16 @@ def load_inputs():
 
 
 def peaks():
-    """(HBM GB/s, bf16 dense TF/s sustained, source). The stage times come from a loop of
-    back-to-back products at the 1 kW power cap, so the sustained GEMM figure applies."""
+    """(HBM GB/s, bf16 dense TF/s burst, bf16 dense TF/s sustained, source). The timed loop of
+    products lasts well under a second, so the burst GEMM figure is the roofline's peak; the
+    sustained one (seconds at the 1 kW power cap) is reported beside it."""
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         with open(path) as f:
             data = json.load(f)
-        return data["hbm_gbs"], data.get("bf16_tflops_sustained", data["bf16_tflops"]), "measured (sustained)"
-    return 6650.0, 1400.0, "fallback (sustained)"
+        return (data["hbm_gbs"], data["bf16_tflops"], data.get("bf16_tflops_sustained", data["bf16_tflops"]),
+                "measured")
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class ClockSampler:
@@ -126,6 +149,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def cpu_scale():
+    """(factor from one sample's time to one full product's, how it was obtained)."""
+    if CPU_FULL_OVER_SAMPLE:
+        return CPU_FULL_OVER_SAMPLE, f"x{CPU_FULL_OVER_SAMPLE:.2f} (full-size/sample time ratio measured on the GPU box)"
+    linear = N / CPU_SAMPLE_N
+    return linear, f"x{linear:g} (linear in N; GMP's superlinear product makes this an underestimate)"
+
+
 def cpu_sample_seconds(sample_n: int, index: int = 0) -> float:
     """One oracle product on the bounded sample (same q width, sample_n coefficients)."""
     oracle = _load("negacyclic_oracle", os.path.join(REPO, "oracle", "oracle.py"))
@@ -174,7 +205,7 @@ def run_reference(args):
 
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
-    scale = N // CPU_SAMPLE_N
+    scale, how = cpu_scale()
     with ctx.Pool(cores) as pool:
         for w in range(args.warmup):
             pool.map(_cpu_worker, [(CPU_SAMPLE_N, w * cores + i) for i in range(cores)])
@@ -194,7 +225,7 @@ def run_reference(args):
         "data": "synthetic", "config": {"workload": WORKLOAD, "sample": f"N={CPU_SAMPLE_N} of {N} coefficients"},
         "cpu_baseline": {"value": value, "unit": "products/s", "cores": cores, "kind": "port",
                          "sample": f"{cores} concurrent GMP Kronecker products of N={CPU_SAMPLE_N}, L={LIMBS} per step,"
-                                   f" scaled by {scale} to one N={N} product"},
+                                   f" each scaled {how} to one N={N} product", "same_config": False},
         "e2e": {"value": value, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -228,6 +259,162 @@ def path_roofline(n: int, limbs: int, info: dict, stage_ms: dict, product_ms: fl
     return {"stages": stages, "roof_ms": round(roof_total, 3), "measured_ms": round(product_ms, 3),
             "measured_over_roof": round(product_ms / roof_total, 3),
             "peaks": {"int8_tops": int8_tops, "hbm_gbs": hbm_gbs}}
+
+
+def fherma_run_leg(args) -> dict:
+    """The headline workload through fherma_run as the platform harness calls it (pageable vectors
+    in, a fresh output vector out): fherma-polynomial-cuda_b200/fherma_timer, a separate process."""
+    binary = os.path.join(PACKAGE_DIR, "fherma_timer")
+    steps = min(args.steps, 5)
+    done = subprocess.run([binary, str(N), str(LIMBS), str(SEED), str(steps), "1"], capture_output=True, text=True,
+                          timeout=900)
+    if done.returncode != 0:
+        return {"error": (done.stderr or done.stdout).strip()[-300:]}
+    result = json.loads(done.stdout.strip().splitlines()[-1])
+    return {"value": 1000.0 / result["median_ms"], "unit": "products/s", "median_ms": result["median_ms"],
+            "mean_ms": result["mean_ms"], "min_ms": result["min_ms"], "max_ms": result["max_ms"],
+            "calls": result["steps"], "init_s": result["init_s"], "commutes": result["commutes"],
+            "api": "fherma_run (include/fherma_b200.h), pageable std::vector operands, fresh output vector per call",
+            "h2d_bytes_per_step": 2 * N * LIMBS * 4, "d2h_bytes_per_step": N * LIMBS * 4}
+
+
+CONFIG2 = (32768, 868, 1, 20)  # N, L, seed of q, instances (operand indices 0..19)
+
+
+def config2_leg(fpc, torch, args) -> dict:
+    """Config 2: N=32768, L=868, q from seed 1, 20 seeded instances: device-resident products/s
+    (every product reads another instance's operands) and end to end through negacyclic_run with
+    page-locked host buffers (each instance's operands copied into them before its timed call)."""
+    n, limbs, seed, count = CONFIG2
+    inputs = load_inputs()
+    t0 = time.perf_counter()
+    instances = [inputs.instance(n, limbs, seed, i) for i in range(count)]
+    gen_s = time.perf_counter() - t0
+    q = instances[0][0]
+    plan = fpc.Plan(n, 32 * limbs, limbs, q)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    dev = [(torch.from_numpy(a.view(np.int32)).cuda(), torch.from_numpy(b.view(np.int32)).cuda())
+           for _, a, b in instances]
+    dc = torch.empty_like(dev[0][0])
+    for da, db in dev[:3]:  # warm-up
+        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for da, db in dev:
+        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sptr)
+    stop.record(stream)
+    stop.synchronize()
+    device_ms = start.elapsed_time(stop) / count
+    status = plan.status()
+    del dev
+    pa = torch.empty((n, limbs), dtype=torch.int32).pin_memory()
+    pb, pc = torch.empty_like(pa).pin_memory(), torch.empty_like(pa).pin_memory()
+    ha, hb, hc = (t.numpy().view(np.uint32) for t in (pa, pb, pc))
+    ha[:], hb[:] = instances[0][1], instances[0][2]
+    plan.run(ha, hb, out=hc)  # warm-up
+    calls = []
+    for _, a, b in instances:
+        ha[:], hb[:] = a, b
+        t1 = time.perf_counter()
+        plan.run(ha, hb, out=hc)
+        calls.append(time.perf_counter() - t1)
+    plan.close()
+    e2e_ms = 1000 * statistics.median(calls)
+    return {"workload": f"N={n}, L={limbs} limbs (27776-bit random odd q, seed {seed}), {count} seeded instances",
+            "device": {"value": 1000.0 / device_ms, "unit": "products/s", "ms_per_product": round(device_ms, 4)},
+            "e2e": {"value": 1000.0 / e2e_ms, "unit": "products/s", "median_ms": round(e2e_ms, 4),
+                    "mean_ms": round(1000 * statistics.mean(calls), 4), "api": "negacyclic_run, page-locked buffers",
+                    "h2d_bytes_per_step": 2 * n * limbs * 4, "d2h_bytes_per_step": n * limbs * 4},
+            "status_word": status, "generation_s": round(gen_s, 1)}
+
+
+# The reference's two ranked points (README.md:9-11): N, W bits; the checker's prime q and stress seeds
+REF_POINTS = [(65536, 1747), (32768, 868)]
+REF_SEEDS = list(range(10001, 10021))  # tools/stress_local.py:16-20: 20 seeds at each ranked point
+REF_BINARIES = [("ordered_streaming", "candidates/ordered-streaming (best ranked entry)"),
+                ("caller_fused_strips", "candidates/caller-fused-strips (fastest measured entry)"),
+                ("harness_b200", "this library: fherma_init/run/free behind the reference's unmodified src/main.cpp")]
+
+
+def refpoints_leg() -> dict:
+    """Per-case fherma_run times of the reference's best entries and of this library, behind the
+    same unmodified harness, at the reference's own points; every output checked against the
+    reference checker's hashes (tests/golden/reference_points.json)."""
+    import hashlib
+    import shutil
+    import tempfile
+
+    ref_dir = os.path.join(REPO, "oracle", "_ref")
+    missing = [name for name, _ in REF_BINARIES if not os.path.exists(os.path.join(ref_dir, name))]
+    if missing:
+        return {"unavailable": f"not built: {', '.join(missing)} (oracle/build_ref.sh needs the reference sources)"}
+    cases = _load("fherma_golden_cases", os.path.join(REPO, "tests", "golden", "cases.py"))
+    with open(os.path.join(REPO, "tests", "golden", "reference_points.json")) as f:
+        golden = json.load(f)["points"]
+    harness = _load("fpc_b200_harness", os.path.join(PACKAGE_DIR, "harness.py"))
+    out = {"seeds": f"{REF_SEEDS[0]}..{REF_SEEDS[-1]}", "timing": "steady_clock around fherma_run (src/main.cpp:181-186)",
+           "points": []}
+    for n, width in REF_POINTS:
+        point = next(p for p in golden if p["N"] == n and p["W"] == width and p["kind"] == "stress_pairs")
+        q, limbs = int(point["q_hex"], 16), point["L"]
+        want = [c["c_sha256"] for c in point["cases"][: len(REF_SEEDS)]]
+        pairs = cases.reference_pairs(n, q, REF_SEEDS, False)
+        arrays = [(np.frombuffer(cases.pack(a, limbs), "<u4").reshape(n, limbs),
+                   np.frombuffer(cases.pack(b, limbs), "<u4").reshape(n, limbs)) for a, b in pairs]
+        root = harness.write_point(tempfile.mkdtemp(prefix="refpoint_"), n, width, limbs,
+                                   np.frombuffer(q.to_bytes(4 * limbs, "little"), "<u4"), arrays)
+        entry = {"N": n, "W_bits": width, "L": limbs}
+        try:
+            for name, what in REF_BINARIES:
+                shutil.rmtree(root / "out", ignore_errors=True)
+                done = subprocess.run([os.path.join(ref_dir, name), str(root)], capture_output=True, text=True,
+                                      timeout=600)
+                result = {"what": what, "rc": done.returncode}
+                if done.returncode == 0:
+                    results = harness.read_results(root)
+                    ms = [1000 * c["seconds"] for c in results["cases"] if c["status"] == "ok"]
+                    hashes = [hashlib.sha256((root / "out" / f"{i:06d}" / "c.bin").read_bytes()).hexdigest()
+                              for i in range(len(pairs))]
+                    result.update(median_ms=round(statistics.median(ms), 4), first_ms=round(ms[0], 4),
+                                  median_after_first_ms=round(statistics.median(ms[1:]), 4),
+                                  min_ms=round(min(ms), 4), init_s=round(results["init_s"], 3),
+                                  cases=len(ms), exact=hashes == want)
+                else:
+                    result["stderr"] = (done.stderr or done.stdout).strip()[-300:]
+                entry[name] = result
+        finally:
+            shutil.rmtree(root, ignore_errors=True)
+        ours, best = entry["harness_b200"], entry["ordered_streaming"]
+        if "median_ms" in ours and "median_ms" in best:
+            entry["ordered_streaming_over_b200"] = round(best["median_ms"] / ours["median_ms"], 3)
+        out["points"].append(entry)
+    out["published_ms"] = {"ordered_streaming": {"65536": 1.0712435, "32768": 0.3752785},
+                           "source": "candidates/ordered-streaming/official-results.json:29,45 (RTX PRO 6000 Blackwell)"}
+    return out
+
+
+def run_cpu_calibrate(args):
+    """One full-size GMP Kronecker product (N=65536, L=1747) and the bounded sample, on one core,
+    back to back: the ratio that scales the sample to a product."""
+    full = cpu_sample_seconds(N, 0)
+    samples = [cpu_sample_seconds(CPU_SAMPLE_N, i) for i in range(3)]
+    sample = statistics.median(samples)
+    print(json.dumps({"mode": "cpu-calibrate", "full_s": round(full, 3), "sample_n": CPU_SAMPLE_N,
+                      "sample_s": [round(x, 3) for x in samples], "full_over_sample": round(full / sample, 3),
+                      "cores": 1, "cpu": _cpu_name()}), flush=True)
+
+
+def _cpu_name() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def run_b200(args):
@@ -330,7 +517,7 @@ def run_b200(args):
                    "plain_value": e2e_value, "setup_s": round(setup_s, 2)}
 
     # --- roofline of the conversion GEMM: 2 ops per byte MAC, M=2N rows, K=4L bytes, 4r weight columns
-    hbm_gbs, bf16_tflops, source = peaks()
+    hbm_gbs, bf16_tflops, bf16_sustained, source = peaks()
     int8_peak = 2 * bf16_tflops  # dense int8 = 2x dense bf16 on B200 (4.5 vs 2.25 PFLOP/s nominal)
     conv_ops = 2.0 * (2 * n_coeff) * (4 * limbs) * (4 * info["primes"])
     crt_ops = 2.0 * n_coeff * (4 * info["primes"]) * (4 * info["words"])
@@ -340,25 +527,40 @@ def run_b200(args):
         "bound": "tensor", "kernel": "gemm_tc_kernel (conversion, tcgen05 kind::i8)",
         "achieved": round(conv_tops, 1), "peak": round(int8_peak, 1), "unit": "TOPS (int8)",
         "frac": round(conv_tops / int8_peak, 4),
+        "frac_of_sustained": round(conv_tops / (2 * bf16_sustained), 4),
+        # ncu sm__pipe_tensor_cycles_active of the conversion GEMM alone (N=16384, L=1747): the
+        # tensor pipe's busy share of cycles, free of the clock under the power cap
+        "tensor_pipe_active_per_cycle": CONVERT_TENSOR_PIPE_ACTIVE,
         "traffic": CONVERT_DRAM_BYTES if (n_coeff, limbs) == (N, LIMBS) else None,
         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
         # operand rows (padded to 32 limbs), conversion weights, residues written
         "algorithmic_bytes_per_launch": float(2 * n_coeff * 4 * padded_limbs + 4 * info["padded_primes"] * 4 * padded_limbs
                                               + 2 * info["primes"] * n_coeff * 4),
-        "peak_source": f"2 x bf16 dense, {source}: {bf16_tflops} TF/s",
+        "peak_source": f"2 x bf16 dense, {source} burst: {bf16_tflops} TF/s (sustained {bf16_sustained})",
         "algorithmic_ops_per_launch": conv_ops,
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "crt_gemm_tops": round(crt_ops / (stage_ms["crt"] / 1000) / 1e12, 1),
         "whole_path": path_roofline(n_coeff, limbs, info, stage_ms, device_ms / args.steps, int8_peak, hbm_gbs),
+        "whole_path_at_sustained": path_roofline(n_coeff, limbs, info, stage_ms, device_ms / args.steps,
+                                                 2 * bf16_sustained, hbm_gbs)["measured_over_roof"],
     }
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        scale = N // CPU_SAMPLE_N
+        scale, how = cpu_scale()
         seconds = cpu_sample_seconds(CPU_SAMPLE_N)
         cpu = {"value": 1.0 / (seconds * scale), "unit": "products/s", "cores": 1, "kind": "port",
                "sample": f"one GMP Kronecker product (the reference checker's algorithm) of N={CPU_SAMPLE_N}, "
-                         f"L={LIMBS}, {seconds:.2f} s, scaled x{scale} to N={N}"}
+                         f"L={LIMBS}, {seconds:.2f} s, scaled {how} to N={N}", "same_config": False}
+
+    extra = {}
+    if rank == 0 and world == 1 and (n_coeff, limbs) == (N, LIMBS):
+        if not args.no_fherma_run:
+            extra["e2e_fherma_run"] = fherma_run_leg(args)
+        if not args.no_config2:
+            extra["config2"] = config2_leg(fpc, torch, args)
+        if not args.no_refpoints:
+            extra["refpoints"] = refpoints_leg()
 
     if rank == 0:
         line = {
@@ -374,6 +576,7 @@ def run_b200(args):
             "batched_e2e": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            **extra,
             "clocks": clocks.summary(),
             "gpu_launches": args.steps * info["kernels_per_product"],
         }
@@ -587,6 +790,19 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def relaunch_under_torchrun(gpus: int) -> int:
+    """`--gpus N` without torchrun: run this same command as N ranks under torch.distributed.run
+    (one process per GPU, rendezvous on 127.0.0.1); returns its exit code."""
+    import socket
+
+    with socket.socket() as probe:
+        probe.bind(("127.0.0.1", 0))
+        port = probe.getsockname()[1]
+    command = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(command).returncode
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -595,12 +811,16 @@ def main():
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     parser.add_argument("--no-batched", action="store_true", help="skip the batched host-array measurement")
+    parser.add_argument("--no-fherma-run", action="store_true", help="skip the fherma_run (pageable) leg")
+    parser.add_argument("--no-config2", action="store_true", help="skip the N=32768, L=868 leg")
+    parser.add_argument("--no-refpoints", action="store_true", help="skip the reference-points comparison")
     parser.add_argument("--workload", default=f"{N},{LIMBS}",
                         help="N,L of a smaller case for profiling (the benchmark line is N=65536,L=1747)")
     parser.add_argument("--device-only", action="store_true",
                         help="device-resident products and stage times only (profiling runs)")
-    parser.add_argument("--mode", choices=("plain", "batch", "serve"), default="plain",
-                        help="plain: the benchmark line; batch / serve: the batched and serving forms")
+    parser.add_argument("--mode", choices=("plain", "batch", "serve", "cpu-calibrate"), default="plain",
+                        help="plain: the benchmark line; batch / serve: the batched and serving forms; "
+                             "cpu-calibrate: one full-size CPU product against the bounded sample")
     parser.add_argument("--count", type=int, default=64, help="batch: number of uneven products")
     parser.add_argument("--lanes", type=int, default=0, help="batch: compute lanes (0 = 1)")
     parser.add_argument("--tune", action="store_true", help="batch: run the autotuner for uncached shapes")
@@ -615,7 +835,14 @@ def main():
     parser.add_argument("--serve-pairs", type=int, default=1, help="serve: operand pairs per (session, N)")
     args = parser.parse_args()
     args.n, args.limbs = (int(x) for x in args.workload.split(","))
-    if args.impl == "reference":
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if world and world != args.gpus:
+        parser.error(f"--gpus {args.gpus} but torchrun started {world} ranks")
+    if not world and args.gpus > 1:
+        sys.exit(relaunch_under_torchrun(args.gpus))
+    if args.mode == "cpu-calibrate":
+        run_cpu_calibrate(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.mode == "batch":
         run_batch(args)

@@ -26,13 +26,15 @@ SHIM_LIBRARY = os.path.join(HERE, "libfherma_negacyclic.so")
 
 OK, EINVAL, ENOFIELDS, ESIZE, ECUDA, ENOMEM, ENODEV = range(7)
 GEMM_AUTO, GEMM_SIMT, GEMM_TENSOR, GEMM_TENSOR_SINGLE = 0, 1, 2, 3
+STATUS_REDUCE, STATUS_GEMM_MASK = 0x1, 0x1ffff00
 
 EXPORTED = [
     "negacyclic_last_error", "negacyclic_init", "negacyclic_get_info", "negacyclic_run",
     "negacyclic_run_device", "negacyclic_free", "negacyclic_host_plan", "negacyclic_debug_read",
     "negacyclic_gemm_u8", "negacyclic_run_device_timed", "negacyclic_work_bytes", "negacyclic_bind_work",
     "negacyclic_pipeline_status", "negacyclic_run_begin", "negacyclic_run_finish",
-    "negacyclic_prepare_host", "negacyclic_run_device_static",
+    "negacyclic_prepare_host", "negacyclic_run_device_static", "negacyclic_plan_status",
+    "negacyclic_gemm_u8_withheld", "negacyclic_batch_status",
     "negacyclic_batch_create", "negacyclic_batch_io", "negacyclic_batch_get_info", "negacyclic_batch_run_device",
     "negacyclic_batch_run", "negacyclic_batch_run_one", "negacyclic_batch_run_plain", "negacyclic_batch_free",
     "negacyclic_server_create", "negacyclic_server_open_session", "negacyclic_server_submit",
@@ -110,6 +112,10 @@ def library() -> ctypes.CDLL:
         lib.negacyclic_run_finish.argtypes = [p, p]
         lib.negacyclic_prepare_host.argtypes = [p]
         lib.negacyclic_run_device_static.argtypes = [p, p, p, p, p]
+        lib.negacyclic_plan_status.argtypes = [p, ctypes.POINTER(u32)]
+        lib.negacyclic_gemm_u8_withheld.argtypes = [p, p, p, u32, u32, u32, u32, ctypes.c_uint64, u32,
+                                                    ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_double)]
+        lib.negacyclic_batch_status.argtypes = [p, p]
         pp = ctypes.POINTER(p)
         lib.negacyclic_batch_create.argtypes = [ctypes.POINTER(PointSpec), u32, ctypes.POINTER(BatchOptions),
                                                 ctypes.POINTER(p)]
@@ -198,6 +204,12 @@ class Plan:
                "negacyclic_run_device_timed")
         return dict(zip(STAGES, list(ms)))
 
+    def status(self) -> int:
+        """The plan's device status word (STATUS_* bits; 0 = sound) after a device sync; clears it."""
+        flags = ctypes.c_uint32()
+        _check(library().negacyclic_plan_status(self.handle, ctypes.byref(flags)), "negacyclic_plan_status")
+        return flags.value
+
     def work_bytes(self) -> int:
         return int(library().negacyclic_work_bytes(self.handle))
 
@@ -234,6 +246,16 @@ def pipeline_status() -> int:
     flags = ctypes.c_uint32()
     _check(library().negacyclic_pipeline_status(ctypes.byref(flags)), "negacyclic_pipeline_status")
     return flags.value
+
+
+def gemm_u8_withheld(a_ptr: int, b_ptr: int, d_ptr: int, m: int, n: int, k: int, engine: int, limit_cycles: int,
+                     withheld_step: int):
+    """(status, flags, elapsed_ms) of the tensor GEMM run with one pipeline stage withheld from the
+    first CTA (pair), every wait bounded by limit_cycles (negacyclic_gemm_u8_withheld)."""
+    flags, ms = ctypes.c_uint32(), ctypes.c_double()
+    status = library().negacyclic_gemm_u8_withheld(a_ptr, b_ptr, d_ptr, m, n, k, engine, limit_cycles, withheld_step,
+                                                   ctypes.byref(flags), ctypes.byref(ms))
+    return status, flags.value, ms.value
 
 
 def host_plan(n: int, limbs: int, q, split: int = 0) -> dict:
@@ -289,6 +311,12 @@ class Batch:
 
     def run_device(self, stream: int = 0):
         _check(library().negacyclic_batch_run_device(self._handle, stream), "negacyclic_batch_run_device")
+
+    def status(self) -> np.ndarray:
+        """Every instance's device status word after a device sync (0 = sound); clears them."""
+        flags = np.zeros(len(self.shapes), np.uint32)
+        _check(library().negacyclic_batch_status(self._handle, flags.ctypes.data), "negacyclic_batch_status")
+        return flags
 
     def run_one(self, index: int, stream: int = 0):
         """Instance `index` alone on `stream` (the plain per-call path)."""

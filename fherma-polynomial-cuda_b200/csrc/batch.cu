@@ -16,7 +16,10 @@
 //     CUDA graph, so a batch run is a single cudaGraphLaunch;
 //   * with host arrays, operand copies run on a copy-in stream and result copies
 //     on a copy-out stream, so instance i's compute overlaps the copy-in of the
-//     instances after it and the copy-out of those before it.
+//     instances after it and the copy-out of those before it;
+//   * each instance has a device status word (NEGACYCLIC_STATUS_*) in one array, cleared at
+//     the start of every run: the blocking host form checks it before returning, and
+//     negacyclic_batch_status reads it after a device run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -153,6 +156,7 @@ struct negacyclic_batch {
     std::vector<cudaStream_t> lanes;
     std::vector<void*> arenas;
     void* io = nullptr;
+    uint32_t* status = nullptr;     // [count] status words, one per instance
     std::vector<size_t> io_offset;  // a, then b, then c per instance
     cudaStream_t capture = nullptr, copy_in = nullptr, copy_out = nullptr;
     std::vector<cudaEvent_t> copied_in, computed;  // per instance, host-array runs
@@ -178,6 +182,7 @@ struct negacyclic_batch {
         if (capture) cudaStreamDestroy(capture);
         for (void* a : arenas) cudaFree(a);
         if (io) cudaFree(io);
+        if (status) cudaFree(status);
         plans.clear();
         cudaSetDevice(previous);
     }
@@ -287,6 +292,9 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
             }
         check(cudaMalloc(&b->io, io_bytes), "cudaMalloc");
         check(cudaMemset(b->io, 0, io_bytes), "cudaMemset");
+        check(cudaMalloc(&b->status, size_t(count) * sizeof(uint32_t)), "cudaMalloc");
+        check(cudaMemset(b->status, 0, size_t(count) * sizeof(uint32_t)), "cudaMemset");
+        for (uint32_t i = 0; i < count; ++i) b->plans[i]->status = b->status + i;
         check(cudaStreamCreateWithFlags(&b->copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&b->copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
         b->copied_in.resize(count);
@@ -303,6 +311,7 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
         for (auto& e : b->joins) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         check(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
         try {
+            check(cudaMemsetAsync(b->status, 0, b->plans.size() * sizeof(uint32_t), b->capture), "cudaMemsetAsync");
             check(cudaEventRecord(b->fork, b->capture), "cudaEventRecord");
             for (uint32_t lane = 0; lane < lanes; ++lane) {
                 check(cudaStreamWaitEvent(b->lanes[lane], b->fork, 0), "cudaStreamWaitEvent");
@@ -378,7 +387,9 @@ int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const ui
         while (order.size() < b->plans.size())
             for (uint32_t lane = 0; lane < b->lanes.size(); ++lane)
                 if (next[lane] < b->lane_order[lane].size()) order.push_back(b->lane_order[lane][next[lane]++]);
-        // copy-in -> compute (the instance's lane) -> copy-out, linked by events
+        // copy-in -> compute (the instance's lane) -> copy-out, linked by events; every lane's first
+        // product waits for a copy-in event recorded after the status words are cleared
+        check(cudaMemsetAsync(b->status, 0, b->plans.size() * sizeof(uint32_t), b->copy_in), "cudaMemsetAsync");
         for (uint32_t i : order) {
             const size_t bytes = b->words(i) * 4;
             check(cudaMemcpyAsync(b->slot(i, 0), a[i], bytes, cudaMemcpyHostToDevice, b->copy_in), "copy a");
@@ -393,9 +404,24 @@ int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const ui
         }
         check(cudaStreamSynchronize(b->copy_out), "batch");
         for (cudaStream_t st : b->lanes) check(cudaStreamSynchronize(st), "batch");
+        std::vector<uint32_t> flags(b->plans.size());
+        check(cudaMemcpy(flags.data(), b->status, flags.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+              "status words");
+        for (uint32_t i = 0; i < flags.size(); ++i)
+            if (flags[i]) return status_failure(flags[i], "batch instance " + std::to_string(i));
     } catch (const CudaError& e) {
         return cuda_failure(e);
     }
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_batch_status(negacyclic_batch* b, uint32_t* flags) {
+    if (!b || !flags) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    DeviceGuard guard(b->device);
+    const size_t bytes = b->plans.size() * sizeof(uint32_t);
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(flags, b->status, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(b->status, 0, bytes) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+        return fail(NEGACYCLIC_ECUDA, cudaGetErrorString(cudaGetLastError()));
     return NEGACYCLIC_OK;
 }
 

@@ -15,9 +15,11 @@
 // Persistent (one CTA per SM) and warp-specialised: warp 0 = TMA producer,
 // warp 1 = MMA issuer and TMEM owner (two 256-column accumulators), warps 2-5 =
 // epilogue, so the epilogue of one tile overlaps the MMAs of the next. Every
-// mbarrier wait is bounded (~2 s of SM clock); on timeout the kernel records an
-// error bit, tells the other roles to stop, waits for what it issued, frees
-// TMEM and returns.
+// mbarrier wait is bounded (TileShape::limit cycles of SM clock, ~2 s by
+// default) and also ends when another role raised the abort flag. On a timeout
+// the kernel records an error bit (in the caller's status word and in a
+// device-wide word), raises the flag (in both CTAs of a pair), lets the
+// copies it issued land, frees TMEM and returns.
 #include <cuda.h>
 
 #include <cstdio>
@@ -37,7 +39,8 @@ constexpr uint32_t kStageBytes = kATileBytes + kBTileBytes;
 constexpr uint32_t kAccColumns = 256;                            // one 128 x 256 s32 accumulator
 constexpr uint32_t kEpilogueWarps = 4;
 constexpr uint32_t kThreads = 64 + 32 * kEpilogueWarps;
-constexpr long long kTimeoutCycles = 4000000000ll;
+constexpr long long kDefaultLimitCycles = 4000000000ll;  // ~2 s at 1.9 GHz
+constexpr uint64_t kAbortDrainNs = 1000000;               // 1 ms: in-flight TMA loads land long before
 constexpr size_t kSmemBytes = size_t(kStages) * kStageBytes + 1024 /*align*/ + 256 /*barriers, TMEM slot*/;
 
 __device__ uint32_t g_tc_error;
@@ -87,13 +90,37 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    long long start = clock64();
+// Bounded wait for the phase with the given parity to complete: false after `limit` cycles, or
+// (when `abort` is given) as soon as another role has raised the abort flag.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit,
+                                          const volatile uint32_t* abort = nullptr) {
+    const long long start = clock64();
     for (uint32_t i = 0;; ++i) {
         if (mbar_try(bar, parity)) return true;
-        if ((i & 255u) == 255u && clock64() - start > kTimeoutCycles) return false;
+        if ((i & 63u) == 63u && ((abort && *abort) || clock64() - start > limit)) return false;
     }
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// After an abort: keep the CTA (and, through the final cluster barrier, its peer) resident for
+// kAbortDrainNs, so that TMA loads still in flight land in live shared memory. The wait is
+// bounded by %globaltimer; a TMA load completes within microseconds.
+__device__ __forceinline__ void abort_drain() {
+    const uint64_t start = global_ns();
+    while (global_ns() - start < kAbortDrainNs) {
+    }
+}
+
+// Records a pipeline error: the device-wide diagnostic word and, when given, the caller's status
+// word (bits shifted into NEGACYCLIC_STATUS_GEMM_MASK).
+__device__ __forceinline__ void record_error(uint32_t* status, uint32_t bit) {
+    atomicOr(&g_tc_error, bit);
+    if (status) atomicOr(status, bit << 8);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
@@ -138,6 +165,9 @@ struct TileShape {
     uint32_t m, columns, k_tiles, m_tiles, n_tiles, group_m;
     RowMap rows;
     uint32_t* tile_counter;  // pair kernel: next unclaimed tile (zero at launch)
+    uint32_t* status;        // caller's status word (NEGACYCLIC_STATUS_*), or nullptr
+    long long limit;         // cycles any one pipeline wait may take
+    uint32_t withheld;       // diagnostics: CTA (pair) 0's producer stops before this pipeline step
 };
 
 // Tile index -> (m tile, n tile) in groups of group_m m-tiles, m fastest, so the
@@ -285,8 +315,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
         if (lane == 0) {
             // ---------------- TMA producer
             uint32_t step = 0, issued = 0;
-            bool ok = true;
-            for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+            bool ok = true, withheld = false;
+            for (uint32_t tile = blockIdx.x; tile < tiles && ok && !withheld; tile += gridDim.x) {
                 uint32_t m_tile, n_tile;
                 tile_coords(tile, shape, m_tile, n_tile);
                 const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
@@ -294,7 +324,11 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 const uint32_t a_row = uint32_t(shape.rows.row(row0));
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kStages, round = step / kStages;
-                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                    if (blockIdx.x == 0 && step == shape.withheld) {  // diagnostics: a stage that never comes
+                        withheld = true;
+                        break;
+                    }
+                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1, shape.limit, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -306,10 +340,11 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
             }
             if (!ok) {
                 *abort_flag = 1;
-                atomicOr(&g_tc_error, 1u);
-                // let the loads already issued land before the CTA can exit
+                record_error(shape.status, 1u);
+                // let the loads already issued land before the CTA can exit (each of these phases
+                // completes: this thread armed it and issued all of its bytes)
                 for (uint32_t st = (issued > kStages ? issued - kStages : 0); st < issued; ++st)
-                    mbar_wait(&full[st % kStages], (st / kStages) & 1);
+                    mbar_wait(&full[st % kStages], (st / kStages) & 1, shape.limit);
             }
         }
     } else if (warp == 1) {
@@ -319,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
             bool ok = true;
             for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++local) {
                 const uint32_t acc = local & 1, use = local >> 1;
-                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1)) {
+                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1, shape.limit, abort_flag)) {
                     ok = false;
                     break;
                 }
@@ -327,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
                 const uint32_t d_tmem = tmem + acc * kAccColumns;
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kStages, round = step / kStages;
-                    if (*abort_flag || !mbar_wait(&full[s], round & 1)) {
+                    if (*abort_flag || !mbar_wait(&full[s], round & 1, shape.limit, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -344,10 +379,10 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
             }
             if (!ok) {
                 *abort_flag = 1;
-                atomicOr(&g_tc_error, 2u);
+                record_error(shape.status, 2u);
             }
             mma_commit(drain);  // arrives once every MMA issued above has completed
-            if (!mbar_wait(drain, 0)) atomicOr(&g_tc_error, 8u);
+            if (!mbar_wait(drain, 0, shape.limit)) record_error(shape.status, 8u);
         }
     } else {
         // ---------------- epilogue: warp w reads TMEM lanes 32*(w%4).. (rows of the tile)
@@ -358,12 +393,12 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_kernel(const __grid_const
             uint32_t m_tile, n_tile;
             tile_coords(tile, shape, m_tile, n_tile);
             const uint32_t row0 = m_tile * kBlockM, col0 = n_tile * kBlockN;
-            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1);
+            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1, shape.limit, abort_flag);
             have = __all_sync(0xffffffffu, have);
             if (!have) {
                 if (lane == 0) {
                     *abort_flag = 1;
-                    atomicOr(&g_tc_error, 4u);
+                    record_error(shape.status, 4u);
                 }
                 break;
             }
@@ -474,8 +509,9 @@ __device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
 }
 
 // Bounded wait with cluster-scope acquire: data written by the other CTA of the pair before its
-// release-arrive on this barrier is visible afterwards.
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) {
+// release-arrive on this barrier is visible afterwards. Ends early once the abort flag is raised.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, long long limit,
+                                                  const volatile uint32_t* abort) {
     const long long start = clock64();
     for (uint32_t i = 0;; ++i) {
         uint32_t ok;
@@ -487,13 +523,20 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
-        if ((i & 255u) == 255u && clock64() - start > kTimeoutCycles) return false;
+        if ((i & 63u) == 63u && (*abort || clock64() - start > limit)) return false;
     }
 }
 
 __device__ __forceinline__ uint32_t peer_address(const void* local) {
     uint32_t remote;
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(1));
+    return remote;
+}
+
+// this CTA's shared-memory word at the same offset in the other CTA of the pair
+__device__ __forceinline__ uint32_t other_address(const void* local, uint32_t rank) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(rank ^ 1u));
     return remote;
 }
 
@@ -526,6 +569,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t rank = cluster_rank();
+    const long long limit = shape.limit;
+    // Raises the abort flag in both CTAs of the pair, so that every role of both ends its waits at
+    // once (the other CTA stays resident until the final cluster barrier, so the store is safe).
+    auto raise_abort = [&](uint32_t bit) {
+        *abort_flag = 1;
+        asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(other_address(const_cast<uint32_t*>(abort_flag), rank)),
+                     "r"(1u)
+                     : "memory");
+        record_error(shape.status, bit);
+    };
     const bool leader = rank == 0;
     const uint32_t tiles = shape.m_tiles * shape.n_tiles;  // m_tiles counts 256-row pair tiles
 
@@ -558,16 +611,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     const uint32_t tmem = *tmem_slot;
     const uint32_t ring_release = leader_address(&ring_empty[0]);  // + slot * 8
 
-    // Reads ring slot i (every reader): the tile index, or `tiles` after a timeout.
+    // Reads ring slot i (every reader): the tile index, or `tiles` after a timeout or an abort.
     auto read_ring = [&](uint32_t i, bool all_lanes_wait) -> uint32_t {
         const uint32_t slot = i % kRing, round = i / kRing;
         bool ok = true;
-        if (all_lanes_wait || lane == 0) ok = !*abort_flag && mbar_wait_cluster(&ring_full[slot], round & 1);
+        if (all_lanes_wait || lane == 0) ok = !*abort_flag && mbar_wait_cluster(&ring_full[slot], round & 1, limit, abort_flag);
         uint32_t tile = ok ? tile_ring[slot] : tiles;
-        if (!ok) {
-            *abort_flag = 1;
-            atomicOr(&g_tc_error, 256u);
-        }
+        if (!ok) raise_abort(256u);
         return tile;
     };
 
@@ -575,12 +625,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             // ---------------- TMA producer (both CTAs): own A half and B half, leader's barrier
             uint32_t step = 0;
-            bool ok = true;
-            for (uint32_t i = 0; ok; ++i) {
+            bool ok = true, withheld = false;
+            for (uint32_t i = 0; ok && !withheld; ++i) {
                 uint32_t tile;
                 if (leader) {  // claim the next tile and publish it to both CTAs
                     const uint32_t slot = i % kRing, round = i / kRing;
-                    if (*abort_flag || !mbar_wait_cluster(&ring_empty[slot], (round & 1) ^ 1)) {
+                    if (*abort_flag || !mbar_wait_cluster(&ring_empty[slot], (round & 1) ^ 1, limit, abort_flag)) {
                         ok = false;
                         // release every reader of this and later slots: they see an end index
                         tile = tiles;
@@ -605,7 +655,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 const uint32_t a_row = uint32_t(shape.rows.row(row0));  // 128 consecutive operand rows
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kPairStages, round = step / kPairStages;
-                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                    if (leader && blockIdx.x == 0 && step == shape.withheld) {  // diagnostics: never armed
+                        withheld = true;
+                        break;
+                    }
+                    if (*abort_flag || !mbar_wait(&empty[s], (round & 1) ^ 1, limit, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -615,10 +669,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     tma_load_2d_pair(b_smem + s * kPairBTileBytes, &b_map, bar, int(ks * kBlockK), int(col0));
                 }
             }
-            if (!ok) {
-                *abort_flag = 1;
-                atomicOr(&g_tc_error, 16u);
-            }
+            if (!ok) raise_abort(16u);
         }
     } else if (warp == 1) {
         if (lane == 0 && leader) {
@@ -630,7 +681,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 mbar_arrive_local(&ring_empty[i % kRing]);
                 if (tile >= tiles) break;
                 const uint32_t acc = local & 1, use = local >> 1;
-                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1)) {
+                if (*abort_flag || !mbar_wait(&acc_empty[acc], (use & 1) ^ 1, limit, abort_flag)) {
                     ok = false;
                     break;
                 }
@@ -638,7 +689,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 const uint32_t d_tmem = tmem + acc * kAccColumns;
                 for (uint32_t ks = 0; ks < shape.k_tiles; ++ks, ++step) {
                     const uint32_t s = step % kPairStages, round = step / kPairStages;
-                    if (*abort_flag || !mbar_wait(&full[s], round & 1)) {
+                    if (*abort_flag || !mbar_wait(&full[s], round & 1, limit, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -653,12 +704,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 }
                 if (ok) mma_commit_pair(&acc_full[acc]);
             }
-            if (!ok) {
-                *abort_flag = 1;
-                atomicOr(&g_tc_error, 32u);
-            }
+            if (!ok) raise_abort(32u);
             mma_commit_pair_local(drain);  // every tcgen05 op here is cta_group::2
-            if (!mbar_wait(drain, 0)) atomicOr(&g_tc_error, 64u);
+            if (!mbar_wait(drain, 0, limit)) raise_abort(64u);
         }
     } else {
         // ---------------- epilogue: this CTA's 128 rows of each pair tile
@@ -678,13 +726,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             uint32_t m_tile, n_tile;
             tile_coords(tile, shape, m_tile, n_tile);
             const uint32_t row0 = m_tile * 256 + rank * kBlockM, col0 = n_tile * kPairBlockN;
-            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1);
+            bool have = !*abort_flag && mbar_wait(&acc_full[acc], use & 1, limit, abort_flag);
             have = __all_sync(0xffffffffu, have);
             if (!have) {
-                if (lane == 0) {
-                    *abort_flag = 1;
-                    atomicOr(&g_tc_error, 128u);
-                }
+                if (lane == 0) raise_abort(128u);
                 break;
             }
             fence_after();
@@ -706,6 +751,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         }
     }
     __syncwarp();
+    // After an abort, TMA loads of either CTA may still be in flight (a producer that stopped does
+    // not know which of the leader's stage barriers will complete): one thread holds this CTA, and
+    // through the barrier below its peer, until they have landed.
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) abort_drain();
     fence_before();
     cluster_sync();  // the leader's MMAs have drained and no peer accesses remain
     if (warp == 1) {
@@ -845,14 +895,17 @@ bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_
 }
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
-                        uint32_t m, bool allow_pairs) {
+                        uint32_t m, bool allow_pairs, long long limit_cycles, uint32_t withheld) {
     const bool pairs = allow_pairs && plan.pairs && (rows.mode == kRowsLinear || rows.span % 256 == 0);
     const uint32_t rows_per_tile = pairs ? 256 : kBlockM;
     const uint32_t m_tiles = (m + rows_per_tile - 1) / rows_per_tile;
     // largest raster group whose A tiles fit comfortably in L2 (~48 MB)
     uint64_t group = (48ull << 20) / (plan.a_tile_bytes * (pairs ? 2 : 1));
     group = group < 4 ? 4 : (group > 64 ? 64 : group);
-    TileShape shape{m, plan.columns, plan.k_tiles, m_tiles, plan.n_tiles, uint32_t(group), rows, plan.tile_counter};
+    TileShape shape{m,      plan.columns,       plan.k_tiles,
+                    m_tiles, plan.n_tiles,      uint32_t(group),
+                    rows,    plan.tile_counter, epilogue.status,
+                    limit_cycles > 0 ? limit_cycles : kDefaultLimitCycles, withheld};
     const uint32_t tiles = m_tiles * plan.n_tiles;
     if (pairs) {
         const uint32_t max_pairs = plan.sm_count / 2;
@@ -867,7 +920,7 @@ void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cu
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
                         uint32_t m) {
-    launch_gemm_tensor(plan, epilogue, stream, rows, m, true);
+    launch_gemm_tensor(plan, epilogue, stream, rows, m, true, 0, kNoWithheldStep);
 }
 
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream) {

@@ -36,9 +36,13 @@ void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cu
 // within the shape the plan was prepared for (see gemm_tensor_accepts).
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
                         uint32_t m);
-// allow_pairs = false forces the single-CTA kernel (diagnostics and tests)
+// allow_pairs = false forces the single-CTA kernel (diagnostics and tests). limit_cycles bounds
+// every pipeline wait (0 = the default, about 2 s of SM clock). withheld (diagnostics only): the
+// producer of the first CTA (pair) stops before this pipeline step, so that its consumer's wait
+// runs out; kNoWithheldStep in normal use.
+constexpr uint32_t kNoWithheldStep = 0xffffffffu;
 void launch_gemm_tensor(const TensorGemmPlan& plan, const Epilogue& epilogue, cudaStream_t stream, const RowMap& rows,
-                        uint32_t m, bool allow_pairs);
+                        uint32_t m, bool allow_pairs, long long limit_cycles, uint32_t withheld);
 bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_t m);
 
 // Device word that records pipeline-wait timeouts of the tensor GEMM (0 = none).

@@ -70,6 +70,9 @@ struct Epilogue {
     //      dots_stride is words rounded up to a multiple of 8 (64-byte rows)
     uint64_t* dots;
     uint32_t words, dots_stride;
+    // every mode: the product's status word (NEGACYCLIC_STATUS_*); the tensor-core kernels set
+    // NEGACYCLIC_STATUS_GEMM_MASK bits in it when a pipeline wait gives up (nullptr: none kept)
+    uint32_t* status;
 };
 
 // a, b: [N][L] -> out: [2][N][Lp], rows split-major (coefficient s*j + t at row op*N + t*N' + j),

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -67,6 +68,7 @@ void enqueue_convert(negacyclic_plan& s, uint32_t t_first, uint32_t t_count, uin
     convert.primes = s.primes;
     convert.r = s.r;
     convert.n = h.n;
+    convert.status = s.status;
     const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span, t_first, t_count);
     const uint32_t m = 2 * t_count * span;
     if (s.convert_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.convert_gemm, rows, m))
@@ -85,6 +87,7 @@ void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t
     crt.dots = s.dots;
     crt.words = h.words;
     crt.dots_stride = s.dots_stride;
+    crt.status = s.status;
     const RowMap rows = RowMap::linear(first);
     if (s.crt_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.crt_gemm, rows, count))
         launch_gemm_tensor(s.crt_gemm, crt, stream, rows, count);
@@ -103,7 +106,7 @@ void enqueue_output(negacyclic_plan& s, uint32_t first, uint32_t count, uint32_t
     reduce.words = h.words;
     reduce.top_shift = h.top_shift;
     reduce.mu_low = h.mu_low;
-    reduce.error_flag = s.error_flag;
+    reduce.error_flag = s.status;
     launch_reduce(reduce, stream);
 }
 
@@ -140,7 +143,7 @@ void enqueue_product(negacyclic_plan& s, uint32_t* d_c, cudaStream_t stream, cud
 
 // Work-space layout of one product (256-byte aligned pieces).
 struct WorkLayout {
-    size_t operands, residues, crt_in, dots, result, error_flag, tile_counter, total;
+    size_t operands, residues, crt_in, dots, result, tile_counter, total;
 };
 
 WorkLayout work_layout(const negacyclic_plan& s) {
@@ -158,8 +161,6 @@ WorkLayout work_layout(const negacyclic_plan& s) {
     at = align(at + size_t(h.n) * s.dots_stride * 8);
     w.result = at;
     at = align(at + size_t(h.n) * h.limbs * 4);
-    w.error_flag = at;
-    at = align(at + 4);
     w.tile_counter = at;  // the tensor-core GEMMs of this work space run one after another
     at = align(at + 4);
     w.total = at;
@@ -177,7 +178,6 @@ std::string bind_work(negacyclic_plan& s, void* arena) {
     s.crt_in = reinterpret_cast<uint32_t*>(base + w.crt_in);
     s.dots = reinterpret_cast<uint64_t*>(base + w.dots);
     s.result = reinterpret_cast<uint32_t*>(base + w.result);
-    s.error_flag = reinterpret_cast<uint32_t*>(base + w.error_flag);
     s.convert_engine = s.crt_engine = NEGACYCLIC_GEMM_SIMT;
     if (!s.gemm_tensor_wanted) return "";
     s.convert_gemm.tile_counter = s.crt_gemm.tile_counter = reinterpret_cast<uint32_t*>(base + w.tile_counter);
@@ -205,6 +205,20 @@ void enqueue_device_product(negacyclic_plan& s, const uint32_t* d_a, const uint3
 
 int cuda_failure(const CudaError& e) {
     return fail(NEGACYCLIC_ECUDA, std::string(e.where) + ": " + cudaGetErrorString(e.code));
+}
+
+int status_failure(uint32_t flags, const std::string& what) {
+    if (!flags) return NEGACYCLIC_OK;
+    char hex[16];
+    std::snprintf(hex, sizeof hex, "0x%x", flags);
+    std::string message = what.empty() ? "" : what + ": ";
+    if (flags & NEGACYCLIC_STATUS_GEMM_MASK)
+        message += "tensor-core GEMM pipeline wait gave up";
+    else if (flags & NEGACYCLIC_STATUS_REDUCE)
+        message += "reduction exceeded its proven correction bound";
+    else
+        message += "device status word set";
+    return fail(NEGACYCLIC_ECUDA, message + " (status " + hex + ")");
 }
 
 
@@ -291,6 +305,8 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         device_alloc(s.crt_weights, size_t(s.crt_columns) * s.k_crt, tables);
         device_alloc(s.q, limbs, tables);
         device_alloc(s.minus_p, limbs, tables);
+        device_alloc(s.own_status, 64, tables);
+        s.status = s.own_status;
         device_alloc(s.crt_words, size_t(s.r) * h.words, work);  // freed once the CRT weights are built
         work = 0;
         s.work_bytes = work_layout(s).total;
@@ -310,6 +326,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         check(cudaMemcpyAsync(s.primes, primes.data(), s.r * sizeof(DevicePrime), cudaMemcpyHostToDevice, st), "upload");
         check(cudaMemcpyAsync(s.q, h.q.data(), limbs * 4, cudaMemcpyHostToDevice, st), "upload q");
         check(cudaMemcpyAsync(s.minus_p, h.minus_p_mod_q.data(), limbs * 4, cudaMemcpyHostToDevice, st), "upload");
+        check(cudaMemsetAsync(s.own_status, 0, 64 * sizeof(uint32_t), st), "memset");
         check(cudaMemcpyAsync(s.crt_words, h.crt_weights.data(), h.crt_weights.size() * 4, cudaMemcpyHostToDevice, st),
               "upload crt");
         launch_twiddles(s.primes, s.r, h.n_sub, s.fwd, s.inv, s.zeta, st);
@@ -336,7 +353,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
             check(cudaMalloc(&probe, 256), "cudaMalloc");
             const std::string why = bind_work(s, probe);
             cudaFree(probe);
-            s.operands = s.residues = s.crt_in = s.result = s.error_flag = nullptr;
+            s.operands = s.residues = s.crt_in = s.result = nullptr;
             s.dots = nullptr;
             if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
         }
@@ -358,6 +375,16 @@ int negacyclic_pipeline_status(uint32_t* flags) {
     if (!word) return fail(NEGACYCLIC_ECUDA, "cannot read the pipeline status word");
     if (cudaMemcpy(flags, word, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemset(word, 0, 4) != cudaSuccess)
+        return fail(NEGACYCLIC_ECUDA, cudaGetErrorString(cudaGetLastError()));
+    return NEGACYCLIC_OK;
+}
+
+int negacyclic_plan_status(negacyclic_plan* s, uint32_t* flags) {
+    if (!s || !flags) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    *flags = 0;
+    DeviceGuard guard(s->device);
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(flags, s->status, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(s->status, 0, 4) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
         return fail(NEGACYCLIC_ECUDA, cudaGetErrorString(cudaGetLastError()));
     return NEGACYCLIC_OK;
 }
@@ -543,7 +570,7 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     const bool a_locked = page_locked(a), b_locked = page_locked(b);
     s.outputs_staged = !(c && page_locked(c));
     if (!a_locked || !b_locked || s.outputs_staged) ensure_staging(s);
-    check(cudaMemsetAsync(s.error_flag, 0, 4, st), "memset");
+    check(cudaMemsetAsync(s.status, 0, 4, st), "memset");
     const uint32_t* src[2] = {a, b};
     const bool locked[2] = {a_locked, b_locked};
     // rows land unpadded (straight in the operands when they need neither padding nor
@@ -644,15 +671,11 @@ int host_finish(negacyclic_plan& s, uint32_t* c) {
             s.team->copy(c + first * h.limbs, s.stage_out + first * h.limbs, size_t(out[k].count) * h.limbs * 4);
         }
     }
-    uint32_t flag = 0, pipeline = 0;
-    check(cudaMemcpyAsync(&flag, s.error_flag, 4, cudaMemcpyDeviceToHost, s.copy_out), "error flag");
-    if (uint32_t* tc = tensor_gemm_error_flag())
-        check(cudaMemcpyAsync(&pipeline, tc, 4, cudaMemcpyDeviceToHost, s.copy_out), "error flag");
     check(cudaStreamSynchronize(s.copy_out), "product");
     check(cudaStreamSynchronize(s.stream), "product");
-    if (flag) return fail(NEGACYCLIC_ECUDA, "reduction exceeded its proven correction bound");
-    if (pipeline) return fail(NEGACYCLIC_ECUDA, "tensor-core GEMM pipeline wait timed out");
-    return NEGACYCLIC_OK;
+    uint32_t flags = 0;  // every kernel that writes the status word ran on s.stream
+    check(cudaMemcpy(&flags, s.status, 4, cudaMemcpyDeviceToHost), "status word");
+    return status_failure(flags);
 }
 
 }  // namespace negacyclic::detail
@@ -684,9 +707,9 @@ int negacyclic_prepare_host(negacyclic_plan* s) {
         host_begin(*s, s->stage_in, s->stage_in + words, nullptr);
         check(cudaStreamSynchronize(s->copy_out), "warm-up");
         check(cudaStreamSynchronize(s->stream), "warm-up");
-        uint32_t flag = 0;
-        check(cudaMemcpy(&flag, s->error_flag, 4, cudaMemcpyDeviceToHost), "warm-up");
-        if (flag) return fail(NEGACYCLIC_ECUDA, "warm-up product reported an error");
+        uint32_t flags = 0;
+        check(cudaMemcpy(&flags, s->status, 4, cudaMemcpyDeviceToHost), "warm-up");
+        if (flags) return status_failure(flags, "warm-up product");
         for (size_t i = 0; i < words; i += 4096)
             if (s->stage_out[i] != 0) return fail(NEGACYCLIC_ECUDA, "warm-up product of zeros is not zero");
     } catch (const CudaError& e) {
@@ -760,7 +783,7 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
             std::string why;
             if (!prepare_gemm_tensor(plan, d_a, k, rows, m, d_b, n, k, why))
                 return fail(NEGACYCLIC_EINVAL, "tensor GEMM unavailable: " + why);
-            launch_gemm_tensor(plan, raw, stream, rows, m, engine == NEGACYCLIC_GEMM_TENSOR);
+            launch_gemm_tensor(plan, raw, stream, rows, m, engine == NEGACYCLIC_GEMM_TENSOR, 0, kNoWithheldStep);
         } else {
             launch_gemm_simt(d_a, k, rows, m, d_b, n, k, raw, stream);
         }
@@ -769,6 +792,55 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
         return cuda_failure(e);
     }
     return NEGACYCLIC_OK;
+}
+
+int negacyclic_gemm_u8_withheld(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uint32_t m, uint32_t n,
+                                uint32_t k, uint32_t engine, uint64_t limit_cycles, uint32_t withheld_step,
+                                uint32_t* flags, double* elapsed_ms) {
+    if (!d_a || !d_b || !d_d || !flags || k % 16 || !m || !n || !k || !limit_cycles || limit_cycles > (1ull << 40))
+        return fail(NEGACYCLIC_EINVAL, "bad GEMM arguments");
+    if (engine != NEGACYCLIC_GEMM_TENSOR && engine != NEGACYCLIC_GEMM_TENSOR_SINGLE)
+        return fail(NEGACYCLIC_EINVAL, "the withheld-stage check applies to the tensor-core engines");
+    *flags = 0;
+    uint32_t* status = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    int result = NEGACYCLIC_OK;
+    try {
+        TensorGemmPlan plan;
+        std::string why;
+        const RowMap rows = RowMap::linear(0);
+        if (!prepare_gemm_tensor(plan, d_a, k, rows, m, d_b, n, k, why))
+            return fail(NEGACYCLIC_EINVAL, "tensor GEMM unavailable: " + why);
+        check(cudaMalloc(&status, sizeof(uint32_t)), "cudaMalloc");
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreate(&start), "cudaEventCreate");
+        check(cudaEventCreate(&stop), "cudaEventCreate");
+        check(cudaMemsetAsync(status, 0, sizeof(uint32_t), stream), "memset");
+        Epilogue raw{};
+        raw.mode = kEpilogueRaw;
+        raw.raw = d_d;
+        raw.raw_ld = n;
+        raw.status = status;
+        check(cudaEventRecord(start, stream), "cudaEventRecord");
+        launch_gemm_tensor(plan, raw, stream, rows, m, engine == NEGACYCLIC_GEMM_TENSOR, (long long)limit_cycles,
+                           withheld_step);
+        check(cudaGetLastError(), "gemm");
+        check(cudaEventRecord(stop, stream), "cudaEventRecord");
+        check(cudaStreamSynchronize(stream), "gemm");
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, start, stop), "cudaEventElapsedTime");
+        if (elapsed_ms) *elapsed_ms = ms;
+        check(cudaMemcpy(flags, status, sizeof(uint32_t), cudaMemcpyDeviceToHost), "status word");
+    } catch (const CudaError& e) {
+        result = cuda_failure(e);
+    }
+    if (start) cudaEventDestroy(start);
+    if (stop) cudaEventDestroy(stop);
+    if (stream) cudaStreamDestroy(stream);
+    if (status) cudaFree(status);
+    if (result == NEGACYCLIC_OK && *flags) result = status_failure(*flags, "GEMM");
+    return result;
 }
 
 }  // extern "C"

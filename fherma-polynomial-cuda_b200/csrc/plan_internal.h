@@ -27,7 +27,10 @@ struct negacyclic_plan {
     // per-product work space: one arena, owned or bound by the caller (batches, servers)
     uint32_t *operands = nullptr, *residues = nullptr, *crt_in = nullptr, *result = nullptr;
     uint64_t* dots = nullptr;
-    uint32_t* error_flag = nullptr;
+    // status word of this plan's products (NEGACYCLIC_STATUS_* bits): the reduce kernel and both
+    // tensor GEMMs set bits in it; allocated with the tables, or pointed into a batch's array
+    uint32_t* status = nullptr;
+    uint32_t* own_status = nullptr;
     void* work_arena = nullptr;  // owned arena (nullptr when the work space is external)
     size_t work_bytes = 0;
     bool gemm_tensor_wanted = true, gemm_tensor_required = false, gemm_pairs_allowed = true;
@@ -52,7 +55,8 @@ struct negacyclic_plan {
         if (stream) cudaStreamSynchronize(stream);
         if (copy_in) cudaStreamSynchronize(copy_in);
         if (copy_out) cudaStreamSynchronize(copy_out);
-        void* buffers[] = {primes, fwd, inv, zeta, convert_weights, crt_weights, q, minus_p, crt_words, work_arena};
+        void* buffers[] = {primes, fwd, inv, zeta, convert_weights, crt_weights, q, minus_p, crt_words, own_status,
+                           work_arena};
         for (void* ptr : buffers)
             if (ptr) cudaFree(ptr);
         for (uint32_t c = 0; c < kMaxChunks; ++c) {
@@ -80,6 +84,9 @@ struct CudaError {
 void check(cudaError_t code, const char* where);
 int fail(int status, const std::string& message);
 int cuda_failure(const CudaError& e);
+// NEGACYCLIC_OK for a zero status word, else NEGACYCLIC_ECUDA with a message naming what failed
+// (`what` prefixes the message, e.g. the batch instance)
+int status_failure(uint32_t flags, const std::string& what = "");
 
 struct DeviceGuard {
     int previous = -1;

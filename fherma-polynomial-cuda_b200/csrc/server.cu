@@ -18,6 +18,9 @@
 // GPU joins the pipeline as soon as a place and memory free up, so its copies overlap their
 // compute. With one compute stream the CTA-pair GEMM kernel is used; concurrent launches of
 // that kernel from several streams stalled, so a process runs one server per device.
+// Each request's product clears its plan's status word first and copies it to a page-locked
+// slot right after (both on the compute stream, so requests of the same plan cannot mix up
+// their words); the completion callback fails the request when the word is nonzero.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -56,6 +59,7 @@ struct Request {
     const uint32_t* b = nullptr;
     uint32_t* c = nullptr;
     double submitted = 0, admitted = 0, finished = 0;
+    uint32_t status_slot = 0;  // index into the server's page-locked status words
     int status = NEGACYCLIC_OK;
     std::string error;
     bool done = false;
@@ -77,6 +81,10 @@ struct negacyclic_server {
     cudaStream_t copy_in = nullptr, compute = nullptr, copy_out = nullptr;
     void* arena = nullptr;  // shared work space, stream-ordered on `compute`
     size_t arena_bytes = 0;
+    // page-locked status words, one per request in flight: request id modulo kStatusSlots (at
+    // most `slots` requests are in flight, admitted and completed in id order)
+    static constexpr uint32_t kStatusSlots = 1024;
+    uint32_t* status_host = nullptr;
     std::vector<cudaEvent_t> spare_events;  // completed events, reusable
     std::vector<cudaEvent_t> all_events;
     std::mutex mu;
@@ -165,6 +173,17 @@ void CUDART_CB negacyclic_server::on_done(void* data) {
     --s->active;
     s->spare_events.push_back(r->copied_in);  // both completed before this callback
     s->spare_events.push_back(r->computed);
+    // the status copy ran on the compute stream before `computed`, which this stream waited for
+    const uint32_t flags = reinterpret_cast<volatile uint32_t*>(s->status_host)[r->status_slot];
+    if (flags) {
+        r->status = NEGACYCLIC_ECUDA;
+        r->error = (flags & NEGACYCLIC_STATUS_GEMM_MASK) ? "tensor-core GEMM pipeline wait gave up"
+                                                          : "reduction exceeded its proven correction bound";
+        ++s->failed;
+        s->finished.notify_all();
+        s->wake.notify_one();
+        return;
+    }
     ++s->completed;
     s->latencies.push_back(r->finished - r->submitted);
     s->last_finish = std::max(s->last_finish, r->finished);
@@ -245,7 +264,12 @@ bool negacyclic_server::admit_one(std::unique_lock<std::mutex>& lock) {
         // only this thread binds plans; kernel arguments are copied at launch
         const std::string why = bind_work(*plan, work);
         if (!why.empty()) throw CudaError{cudaErrorInvalidValue, "bind_work"};
+        r->status_slot = uint32_t(r->id % kStatusSlots);
+        check(cudaMemsetAsync(plan->status, 0, sizeof(uint32_t), compute), "cudaMemsetAsync");
         enqueue_device_product(*plan, d_a, d_b, d_c, compute);
+        check(cudaMemcpyAsync(status_host + r->status_slot, plan->status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              compute),
+              "status word");
         check(cudaEventRecord(r->computed, compute), "cudaEventRecord");
         check(cudaStreamWaitEvent(copy_out, r->computed, 0), "cudaStreamWaitEvent");
         check(cudaMemcpyAsync(r->c, d_c, words * 4, cudaMemcpyDeviceToHost, copy_out), "copy c");
@@ -288,10 +312,14 @@ int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_s
     s->device = device;
     s->budget = o.hbm_budget ? o.hbm_budget : (uint64_t(60) << 30);
     s->slots = o.slots ? o.slots : 4;
+    if (s->slots > negacyclic_server::kStatusSlots) return fail(NEGACYCLIC_EINVAL, "at most 1024 slots");
     DeviceGuard guard(device);
     try {
         for (cudaStream_t* st : {&s->copy_in, &s->compute, &s->copy_out})
             check(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaHostAlloc(reinterpret_cast<void**>(&s->status_host), negacyclic_server::kStatusSlots * sizeof(uint32_t),
+                            cudaHostAllocDefault),
+              "cudaHostAlloc");
         // keep freed request memory in the pool up to the budget instead of returning it
         cudaMemPool_t pool = nullptr;
         check(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
@@ -300,6 +328,7 @@ int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_s
     } catch (const CudaError& e) {
         for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
             if (st) cudaStreamDestroy(st);
+        if (s->status_host) cudaFreeHost(s->status_host);
         return cuda_failure(e);
     }
     negacyclic_server* raw = s.release();
@@ -416,6 +445,7 @@ void negacyclic_server_free(negacyclic_server* s) {
         for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
             if (st) cudaStreamSynchronize(st);
         if (s->arena) cudaFree(s->arena);
+        if (s->status_host) cudaFreeHost(s->status_host);
         for (cudaEvent_t e : s->all_events) cudaEventDestroy(e);
         for (cudaStream_t st : {s->copy_in, s->compute, s->copy_out})
             if (st) cudaStreamDestroy(st);

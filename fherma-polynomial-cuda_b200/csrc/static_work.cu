@@ -11,24 +11,29 @@
 // only the parameter tables, and then multiply through this entry point.
 //
 // The work space (padded operands, residues, CRT inputs and word sums, the result
-// staging and the error word) is g_static_work below: 64 MiB, enough for products up
-// to about N = 8192 with L = 128, or N = 4096 with L = 256. A point whose work space is
-// larger is rejected with an error that names both sizes.
+// staging and the GEMM tile counter) is g_static_work below: 64 MiB, enough for
+// products up to about N = 8192 with L = 128, or N = 4096 with L = 256. A point whose
+// work space is larger is rejected with an error that names both sizes.
 //
 // In host code g_static_work is only a stand-in for the array. Its device address
-// comes from cudaGetSymbolAddress, called once per device with that device current,
-// on the first call of this entry point on that device. That first call loads this
-// file's module and so sets aside the array, which stays until the process exits.
-// Make that first call before any stream capture.
+// comes from cudaGetSymbolAddress, called with the device current on the first call
+// of this entry point on that device (and again if the device's context was made
+// anew, e.g. after cudaDeviceReset). That first call loads this file's module and so
+// sets aside the array, which stays until the process exits. Make that first call
+// before any stream capture. Under CUDA_MODULE_LOADING=EAGER the driver loads the
+// module, and sets aside the 64 MiB, on every device when the context is created,
+// whether or not this entry point is ever called.
 //
 // Every call shares the one array and leaves its contents behind:
-//  * the error word, the only piece a product needs to start at zero, is cleared at
-//    the start of each call;
+//  * nothing in it needs to start at zero: the GEMM tile counter is cleared before
+//    each GEMM, and the status word that reports device-side errors belongs to the
+//    plan (read it with negacyclic_plan_status);
 //  * padding limbs and padding prime columns meet zero weights in the GEMMs, so
 //    whatever they hold never reaches the result;
 //  * two calls whose work overlaps on the GPU (different streams, or different host
 //    threads without ordering between them) overwrite each other's intermediates and
 //    return wrong products; order such calls on one stream or with events.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -49,29 +54,58 @@ static __device__ __align__(256) unsigned char g_static_work[kStaticWorkBytes];
 
 std::mutex g_static_mutex;
 void* g_static_address[kMaxDevices] = {};
+unsigned long long g_static_context[kMaxDevices] = {};  // context the address belongs to
 
-// Device address of g_static_work on `device` (looked up once per device; the caller has made
-// `device` current).
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (0 if the driver cannot tell): a context made
+// anew for the device gets a new id, and the array's address must then be looked up again.
+unsigned long long current_context_id() {
+    static CtxGetCurrent get_current = nullptr;
+    static CtxGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult found{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrent>(fn);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetId>(fn);
+    });
+    CUcontext context = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&context) != CUDA_SUCCESS || !context ||
+        get_id(context, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of g_static_work on `device`, which the caller has made current: looked up once
+// per device and context.
 void* static_work_address(int device) {
     std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_address[device]) {
+    const unsigned long long context = current_context_id();
+    if (!g_static_address[device] || context == 0 || context != g_static_context[device]) {
         void* ptr = nullptr;
         check(cudaGetSymbolAddress(&ptr, g_static_work), "cudaGetSymbolAddress(static work space)");
         g_static_address[device] = ptr;
+        g_static_context[device] = context;
     }
     return g_static_address[device];
 }
 
 // The plan fields that bind_work rewrites, so the plan's own binding can be put back.
 struct Binding {
-    uint32_t *operands, *residues, *crt_in, *result, *error_flag;
+    uint32_t *operands, *residues, *crt_in, *result;
     uint64_t* dots;
     uint32_t convert_engine, crt_engine;
     TensorGemmPlan convert_gemm, crt_gemm;
 
     explicit Binding(const negacyclic_plan& s)
-        : operands(s.operands), residues(s.residues), crt_in(s.crt_in), result(s.result),
-          error_flag(s.error_flag), dots(s.dots), convert_engine(s.convert_engine), crt_engine(s.crt_engine),
+        : operands(s.operands), residues(s.residues), crt_in(s.crt_in), result(s.result), dots(s.dots), convert_engine(s.convert_engine), crt_engine(s.crt_engine),
           convert_gemm(s.convert_gemm), crt_gemm(s.crt_gemm) {}
 
     void restore(negacyclic_plan& s) const {
@@ -79,7 +113,6 @@ struct Binding {
         s.residues = residues;
         s.crt_in = crt_in;
         s.result = result;
-        s.error_flag = error_flag;
         s.dots = dots;
         s.convert_engine = convert_engine;
         s.crt_engine = crt_engine;
@@ -109,7 +142,6 @@ extern "C" int negacyclic_run_device_static(negacyclic_plan* s, const uint32_t* 
             own.restore(*s);
             return fail(NEGACYCLIC_EINVAL, why);
         }
-        check(cudaMemsetAsync(s->error_flag, 0, sizeof(uint32_t), stream), "clear error word");
         // kernel arguments (pointers, tensor maps) are copied at launch, so the plan's own
         // binding can be put back as soon as the product is enqueued
         enqueue_device_product(*s, d_a, d_b, d_c, stream);

@@ -84,41 +84,59 @@ def instance(n: int, limbs: int, seed: int, index: int = 0):
     return q, a, b
 
 
-def edge_operands(n: int, q: np.ndarray) -> dict[str, np.ndarray]:
-    """Edge inputs: zero, unit, all q-1, impulses, alternating q-1/q-2, carry boundaries."""
+EDGE_NAMES = ("zero", "ones", "max", "impulse0", "impulse_last", "alternating", "alt_zero", "carry",
+              "boundary", "half", "half_up")
+
+
+def edge_operand(n: int, q: np.ndarray, name: str) -> np.ndarray:
+    """One edge input: zero, unit, all q-1, impulses, alternating q-1/q-2, carry boundaries."""
     limbs = q.shape[0]
     qi = to_int(q)
     zero = np.zeros((n, limbs), dtype=np.uint32)
-    ones = zero.copy()
-    ones[:, 0] = 1 if qi > 1 else 0
-    maximum = np.tile(from_int(qi - 1, limbs), (n, 1))
-    impulse0 = zero.copy()
-    impulse0[0] = from_int(1 % qi, limbs)
-    impulse_last = zero.copy()
-    impulse_last[-1] = from_int(qi - 1, limbs)
-    alternating = maximum.copy()
-    alternating[1::2] = from_int(max(qi - 2, 0), limbs)
-    alt_zero = zero.copy()  # q-1 at odd indices, 0 at even (tools/stress_local.py:25)
-    alt_zero[1::2] = from_int(qi - 1, limbs)
-    # 0xFFFFFFFF limbs where the value stays below q: all-ones below q's top limb,
-    # and q's top limb minus one on top (or all-ones on q-1's top when that is 0).
-    ff = np.full(limbs, 0xFFFFFFFF, dtype=np.uint32)
-    top = int(q[-1])
-    if top > 1:
-        ff[-1] = top - 1
-        below = ff
-    else:
-        below = from_int(qi - 1, limbs)
-    carry = np.tile(below, (n, 1))
-    # limb-boundary values min(q-1, 2^(32*(i mod L + 1)) - 1) (tools/stress_local.py:26)
-    boundary = poly_from_ints([min(qi - 1, (1 << (32 * (i % limbs + 1))) - 1) for i in range(n)], limbs)
-    half = np.tile(from_int(qi // 2, limbs), (n, 1))
-    half_up = np.tile(from_int((qi // 2 + 1) % qi, limbs), (n, 1))
-    return {
-        "zero": zero, "ones": ones, "max": maximum, "impulse0": impulse0,
-        "impulse_last": impulse_last, "alternating": alternating, "alt_zero": alt_zero, "carry": carry,
-        "boundary": boundary, "half": half, "half_up": half_up,
-    }
+    if name == "zero":
+        return zero
+    if name == "ones":
+        zero[:, 0] = 1 if qi > 1 else 0
+        return zero
+    if name == "max":
+        return np.tile(from_int(qi - 1, limbs), (n, 1))
+    if name == "impulse0":
+        zero[0] = from_int(1 % qi, limbs)
+        return zero
+    if name == "impulse_last":
+        zero[-1] = from_int(qi - 1, limbs)
+        return zero
+    if name == "alternating":  # q-1 at even indices, q-2 at odd ones
+        out = np.tile(from_int(qi - 1, limbs), (n, 1))
+        out[1::2] = from_int(max(qi - 2, 0), limbs)
+        return out
+    if name == "alt_zero":  # q-1 at odd indices, 0 at even (tools/stress_local.py:25)
+        zero[1::2] = from_int(qi - 1, limbs)
+        return zero
+    if name == "carry":
+        # 0xFFFFFFFF limbs where the value stays below q: all-ones below q's top limb,
+        # and q's top limb minus one on top (or all-ones on q-1's top when that is 0).
+        ff = np.full(limbs, 0xFFFFFFFF, dtype=np.uint32)
+        top = int(q[-1])
+        if top > 1:
+            ff[-1] = top - 1
+            below = ff
+        else:
+            below = from_int(qi - 1, limbs)
+        return np.tile(below, (n, 1))
+    if name == "boundary":  # min(q-1, 2^(32*(i mod L + 1)) - 1) (tools/stress_local.py:26)
+        rows = np.stack([from_int(min(qi - 1, (1 << (32 * (j + 1))) - 1), limbs) for j in range(min(limbs, n))])
+        return rows[np.arange(n) % limbs] if n else zero
+    if name == "half":
+        return np.tile(from_int(qi // 2, limbs), (n, 1))
+    if name == "half_up":
+        return np.tile(from_int((qi // 2 + 1) % qi, limbs), (n, 1))
+    raise KeyError(name)
+
+
+def edge_operands(n: int, q: np.ndarray) -> dict[str, np.ndarray]:
+    """Every edge input of `edge_operand`, by name."""
+    return {name: edge_operand(n, q, name) for name in EDGE_NAMES}
 
 
 EDGE_PAIRS = [

@@ -41,6 +41,12 @@ extern "C" {
 #define NEGACYCLIC_ENOMEM 5     /* device or pinned host allocation failed */
 #define NEGACYCLIC_ENODEV 6     /* no usable sm_100 device */
 
+/* Bits of a plan's device status word (negacyclic_plan_status, negacyclic_batch_status). The
+ * reference has no device-side error word: its waits are unbounded and its reduction has no
+ * bound to exceed (src/solve.cu:468-490). */
+#define NEGACYCLIC_STATUS_REDUCE 0x1u           /* a coefficient needed more corrections than proven */
+#define NEGACYCLIC_STATUS_GEMM_MASK 0x1ffff00u  /* a tensor-core GEMM pipeline wait gave up (which role: bits) */
+
 /* GEMM engine for the two byte-sliced products (conversion and CRT). */
 #define NEGACYCLIC_GEMM_AUTO 0   /* tensor cores where the shape allows it */
 #define NEGACYCLIC_GEMM_SIMT 1   /* dp4a CUDA-core kernel (any shape) */
@@ -120,7 +126,9 @@ int negacyclic_run_finish(negacyclic_plan* plan, uint32_t* c);
 /*
  * Device-resident product: d_a, d_b, d_c are device arrays of n*limbs words on
  * the plan's device. Enqueued on `stream` (a cudaStream_t; NULL = the legacy
- * default stream) and returns without waiting.
+ * default stream) and returns without waiting. Device-side failures (a GEMM
+ * pipeline wait that gave up, a reduction beyond its proven bound) set bits in
+ * the plan's status word, which negacyclic_plan_status reads.
  */
 int negacyclic_run_device(negacyclic_plan* plan, const uint32_t* d_a, const uint32_t* d_b,
                           uint32_t* d_c, void* stream);
@@ -132,6 +140,15 @@ int negacyclic_run_device(negacyclic_plan* plan, const uint32_t* d_a, const uint
  */
 int negacyclic_run_device_timed(negacyclic_plan* plan, const uint32_t* d_a, const uint32_t* d_b,
                                 uint32_t* d_c, void* stream, float* stage_ms);
+
+/*
+ * Waits for the plan's device (cudaDeviceSynchronize), then stores the plan's
+ * status word in *flags (NEGACYCLIC_STATUS_* bits; 0 = every product since the
+ * last read was sound) and clears it. The device entry points, including
+ * negacyclic_run_device_static, only ever set bits in the word; negacyclic_run
+ * clears it when it starts and fails with NEGACYCLIC_ECUDA when it ends nonzero.
+ */
+int negacyclic_plan_status(negacyclic_plan* plan, uint32_t* flags);
 
 /* Bytes of device work space one product of this plan needs (operands, residues, CRT
  * inputs and word sums, result). */
@@ -158,22 +175,43 @@ int negacyclic_bind_work(negacyclic_plan* plan, void* d_work, size_t bytes);
  * Make the plan at start-up with external_work = 1 (tables only). Points whose
  * negacyclic_work_bytes() exceeds the array are rejected (NEGACYCLIC_EINVAL, the
  * message names both sizes); 64 MiB holds e.g. N = 8192 with L = 128. The plan's
- * own work-space binding is left as it was.
+ * own work-space binding is left as it was. Device-side errors go to the plan's
+ * status word (negacyclic_plan_status), which lives with the plan's tables.
  * The first call on a device looks up the array's address (and makes the driver
- * load it); make that first call before any stream capture. All calls share the
- * array: calls whose work overlaps on the GPU (other streams, unordered threads)
- * race and corrupt each other, so order them on one stream or with events.
+ * load it); make that first call before any stream capture. Under
+ * CUDA_MODULE_LOADING=EAGER the driver instead loads it, and so reserves the
+ * 64 MiB, on every device when the process's context is created, whether or not
+ * this entry point is called. All calls share the array: calls whose work
+ * overlaps on the GPU (other streams, unordered threads) race and corrupt each
+ * other, so order them on one stream or with events.
  */
 #define NEGACYCLIC_STATIC_WORK_BYTES ((size_t)64 << 20)
 int negacyclic_run_device_static(negacyclic_plan* plan, const uint32_t* d_a, const uint32_t* d_b,
                                  uint32_t* d_c, void* stream);
 
 /*
- * Diagnostics of the current device: *flags receives the tensor-core GEMM status
- * word (nonzero = a pipeline wait gave up after ~2 s since the last call; bits say
- * which role) and the word is cleared. Synchronises the device.
+ * Diagnostics of the current device: *flags receives the device-wide tensor-core
+ * GEMM word (nonzero = a pipeline wait of any GEMM gave up since the last call;
+ * bits say which role) and the word is cleared. Synchronises the device. Each
+ * product also reports its own failures in its plan's status word.
  */
 int negacyclic_pipeline_status(uint32_t* flags);
+
+/*
+ * Diagnostic of the tensor-core GEMM's failure path, with no counterpart in the
+ * reference (its waits have no bound). Runs the raw GEMM of negacyclic_gemm_u8
+ * (engine NEGACYCLIC_GEMM_TENSOR or _TENSOR_SINGLE) with every pipeline wait
+ * bounded by limit_cycles of SM clock, on a stream of its own, and with the TMA
+ * producer of the first CTA (pair) stopping before pipeline step withheld_step
+ * (0xffffffff: never), so that the stage its MMA issuer waits for never arrives.
+ * The wait runs out, every role of that CTA (pair) stops, and the kernel returns;
+ * *flags receives the status word (NEGACYCLIC_STATUS_GEMM_MASK bits) and
+ * *elapsed_ms the kernel's device time. Returns NEGACYCLIC_ECUDA when flags is
+ * nonzero. Blocking. d_d is left partly unwritten on failure.
+ */
+int negacyclic_gemm_u8_withheld(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uint32_t m, uint32_t n,
+                                uint32_t k, uint32_t engine, uint64_t limit_cycles, uint32_t withheld_step,
+                                uint32_t* flags, double* elapsed_ms);
 
 /* Releases the plan and every device/pinned buffer it holds. NULL is a no-op. */
 void negacyclic_free(negacyclic_plan* plan);
@@ -247,15 +285,21 @@ int negacyclic_batch_io(negacyclic_batch* batch, uint32_t index, uint32_t** d_a,
 int negacyclic_batch_get_info(const negacyclic_batch* batch, uint32_t index,
                               negacyclic_batch_instance* info);
 
-/* Every product of the batch from its device buffers: one cudaGraphLaunch on `stream`. */
+/* Every product of the batch from its device buffers: one cudaGraphLaunch on `stream`. The
+ * graph first clears every instance's status word; read them with negacyclic_batch_status. */
 int negacyclic_batch_run_device(negacyclic_batch* batch, void* stream);
+
+/* Waits for the device, then stores each instance's status word in flags[0..count) (0 = sound;
+ * NEGACYCLIC_STATUS_* bits otherwise) and clears them. */
+int negacyclic_batch_status(negacyclic_batch* batch, uint32_t* flags);
 
 /* Instance `index` alone, as one plain product (the per-call path), enqueued on `stream`.
  * Must not overlap other runs of the same batch (instances share lane work spaces). */
 int negacyclic_batch_run_one(negacyclic_batch* batch, uint32_t index, void* stream);
 
 /* Host arrays a[i], b[i], c[i] per instance: copy-in, compute and copy-out streams overlap
- * (instance i computes while later operands copy in and earlier results copy out). Blocking. */
+ * (instance i computes while later operands copy in and earlier results copy out). Blocking;
+ * fails with NEGACYCLIC_ECUDA, naming the instance, when an instance's status word is set. */
 int negacyclic_batch_run(negacyclic_batch* batch, const uint32_t* const* a, const uint32_t* const* b,
                          uint32_t* const* c);
 
@@ -305,7 +349,8 @@ int negacyclic_server_open_session(negacyclic_server* server, uint32_t w, uint32
 int negacyclic_server_submit(negacyclic_server* server, uint32_t session, uint32_t n,
                              const uint32_t* a, const uint32_t* b, uint32_t* c, uint64_t* request);
 
-/* Blocks until the request finished (or timeout_ms passed; <= 0 waits without limit). */
+/* Blocks until the request finished (or timeout_ms passed; <= 0 waits without limit). A request
+ * whose product set its plan's status word fails with NEGACYCLIC_ECUDA. */
 int negacyclic_server_wait(negacyclic_server* server, uint64_t request, double timeout_ms,
                            double* latency_ms);
 

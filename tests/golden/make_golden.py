@@ -1,8 +1,8 @@
 """Writes tests/golden/*.json from the reference's own checker code.
 
-Run in a checkout that has the reference at REFERENCE (default /root/reference):
+Run with REFERENCE set to a checkout of the reference project (required):
 
-    python tests/golden/make_golden.py [--big]
+    REFERENCE=<checkout> python tests/golden/make_golden.py [--big --jobs J]
 
 It imports the reference's tests/reference.py and calls its `save_point`,
 `kronecker` and `modulus` functions. That module imports gmpy2, which this
@@ -13,13 +13,18 @@ bases. Nothing else of the reference is changed or copied.
 
 Outputs (hashes of the reference's bytes; full values only for tiny points):
   reference_points.json  tools/validate_local.py:13-14 points, tools/stress_local.py:16 points
-  baseline_cfg.json      the N=4096/L=64 random-odd-q product and its edge pairs
-                         (--big adds one N=32768/L=868 and one N=65536/L=1747 instance)
+  baseline_cfg.json      the N=4096/L=64 random-odd-q product and its edge pairs; --big adds
+                         N=32768/L=868 (q from seed 1, operand indices 0..19, every edge pair)
+                         and N=65536/L=1747 (seeds 2..21, one instance each; every edge pair
+                         with the seed-2 q). The big products run in parallel worker processes
+                         (--jobs; about 10 GB of memory each at N=65536/L=1747) and are cached
+                         in --cache as they finish, so an interrupted run resumes.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes
+import multiprocessing
 import importlib.util
 import json
 import os
@@ -34,7 +39,7 @@ REPO = HERE.parents[1]
 sys.path.insert(0, str(HERE))
 import cases  # noqa: E402
 
-REFERENCE = Path(os.environ.get("REFERENCE", "/root/reference"))
+REFERENCE = Path(os.environ["REFERENCE"]) if os.environ.get("REFERENCE") else None
 
 _gmp = ctypes.CDLL("libgmp.so.10")
 
@@ -76,6 +81,8 @@ class _Mpz(int):
 
 
 def load_reference():
+    if REFERENCE is None or not (REFERENCE / "tests/reference.py").exists():
+        raise SystemExit("set REFERENCE to a checkout of the reference project (it must hold tests/reference.py)")
     stand_in = types.ModuleType("gmpy2")
     stand_in.mpz = _Mpz
     stand_in.is_prime = lambda n, reps=25: cases.is_probable_prime(int(n))
@@ -117,8 +124,8 @@ def validate_points(ref):
                        "seeds": [101, 202], "edge_cases": True,
                        "cases": record(n, width, limbs, q, pairs, outputs)})
         print(json.dumps({"N": n, "W": width, "cases": len(outputs), "s": round(time.time() - started, 1)}), flush=True)
-    # tools/stress_local.py:16-27 (4 seeds at the two small stress points, 2 at the ranked points)
-    for n, width, count in [(128, 4096, 4), (131072, 128, 4), (32768, 868, 2), (65536, 1747, 2)]:
+    # tools/stress_local.py:16-27 (4 seeds at the two small stress points, 20 at the ranked points)
+    for n, width, count in [(128, 4096, 4), (131072, 128, 4), (32768, 868, 20), (65536, 1747, 20)]:
         started = time.time()
         q = int(ref.modulus(n, width))
         limbs = (width + 31) // 32
@@ -132,44 +139,86 @@ def validate_points(ref):
     return points
 
 
-def baseline_points(ref, big):
+def _instance_task(task):
+    """One big product through the reference's kronecker, in a worker process."""
+    n, limbs, seed, label = task
     sys.path.insert(0, str(REPO / "fherma-polynomial-cuda_b200"))
     import inputs  # the package's seeded generator (numpy)
-    configs = [(4096, 64, 0, [0], True)]
+    ref = load_reference()
+    started = time.time()
+    if label.startswith("seed"):
+        q, a, b = inputs.instance(n, limbs, seed, int(label.split("index")[1]))
+    else:
+        q = inputs.random_modulus(limbs, seed)
+        x, y = _edge_names(inputs, label)
+        a, b = inputs.edge_operand(n, q, x), inputs.edge_operand(n, q, y)
+    entry = {"label": label,
+             "a_sha256": cases.sha256(a.astype("<u4").tobytes()),
+             "b_sha256": cases.sha256(b.astype("<u4").tobytes())}
+    qi = inputs.to_int(q)
+    a, b = inputs.poly_to_ints(a), inputs.poly_to_ints(b)
+    c = ref.kronecker(a, b, qi)
+    del a, b
+    entry["c_sha256"] = cases.sha256(cases.pack(c, limbs))
+    return {"N": n, "L": limbs, "seed": seed, "q_hex": hex(qi), "entry": entry, "s": round(time.time() - started, 1)}
+
+
+def _edge_names(inputs, label):
+    for x, y in inputs.EDGE_PAIRS:
+        if label == f"edge_{x}_{y}":
+            return x, y
+    raise KeyError(label)
+
+
+def _point_tasks(n, limbs, seed, instances, edges):
+    sys.path.insert(0, str(REPO / "fherma-polynomial-cuda_b200"))
+    import inputs
+    tasks = [(n, limbs, s, f"seed{s}_index{i}") for s, i in instances]
+    if edges:
+        tasks += [(n, limbs, seed, f"edge_{x}_{y}") for x, y in inputs.EDGE_PAIRS]
+    return tasks
+
+
+def baseline_points(big, jobs, cache_path):
+    # (N, L, seed of the edge pairs' q, [(seed, operand index)], edges)
+    configs = [(4096, 64, 0, [(0, 0)], True)]
     if big:
-        configs += [(32768, 868, 1, [0], False), (65536, 1747, 2, [0], False)]
-    points = []
-    for n, limbs, seed, indices, edges in configs:
-        started = time.time()
-        entries = []
-        for index in indices:
-            q, a, b = inputs.instance(n, limbs, seed, index)
-            qi = inputs.to_int(q)
-            c = ref.kronecker(inputs.poly_to_ints(a), inputs.poly_to_ints(b), qi)
-            entries.append({"label": f"seed{seed}_index{index}",
-                            "a_sha256": cases.sha256(a.astype("<u4").tobytes()),
-                            "b_sha256": cases.sha256(b.astype("<u4").tobytes()),
-                            "c_sha256": cases.sha256(cases.pack(c, limbs))})
-        if edges:
-            q = inputs.random_modulus(limbs, seed)
-            qi = inputs.to_int(q)
-            ops = inputs.edge_operands(n, q)
-            for x, y in inputs.EDGE_PAIRS:
-                c = ref.kronecker(inputs.poly_to_ints(ops[x]), inputs.poly_to_ints(ops[y]), qi)
-                entries.append({"label": f"edge_{x}_{y}",
-                                "a_sha256": cases.sha256(ops[x].astype("<u4").tobytes()),
-                                "b_sha256": cases.sha256(ops[y].astype("<u4").tobytes()),
-                                "c_sha256": cases.sha256(cases.pack(c, limbs))})
-        points.append({"N": n, "L": limbs, "seed": seed, "q_hex": hex(inputs.to_int(inputs.random_modulus(limbs, seed))),
-                       "cases": entries})
-        print(json.dumps({"N": n, "L": limbs, "cases": len(entries), "s": round(time.time() - started, 1)}), flush=True)
-    return points
+        configs += [(32768, 868, 1, [(1, i) for i in range(20)], True),
+                    (65536, 1747, 2, [(s, 0) for s in range(2, 22)], True)]
+    tasks = [t for n, limbs, seed, inst, edges in configs for t in _point_tasks(n, limbs, seed, inst, edges)]
+    done = {}
+    cache = Path(cache_path)
+    if cache.exists():
+        for line in cache.read_text().splitlines():
+            item = json.loads(line)
+            done[(item["N"], item["L"], item["seed"], item["entry"]["label"])] = item
+    todo = sorted((t for t in tasks if t not in done), key=lambda t: -t[0] * t[1])
+    if todo:
+        context = multiprocessing.get_context("spawn")
+        with context.Pool(jobs, maxtasksperchild=1) as pool, cache.open("a") as log:
+            for item in pool.imap_unordered(_instance_task, todo):
+                done[(item["N"], item["L"], item["seed"], item["entry"]["label"])] = item
+                log.write(json.dumps(item) + "\n")
+                log.flush()
+                print(json.dumps({"N": item["N"], "L": item["L"], "seed": item["seed"],
+                                  "label": item["entry"]["label"], "s": item["s"]}), flush=True)
+    points = {}
+    for task in tasks:  # one point per (N, L, q seed), cases in task order
+        item = done[task]
+        key = (item["N"], item["L"], item["seed"])
+        if key not in points:
+            points[key] = {"N": item["N"], "L": item["L"], "seed": item["seed"], "q_hex": item["q_hex"], "cases": []}
+        points[key]["cases"].append(item["entry"])
+    return list(points.values())
 
 
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--big", action="store_true", help="add the N=32768/L=868 and N=65536/L=1747 products")
     parser.add_argument("--only", choices=("reference", "baseline"), default=None)
+    parser.add_argument("--jobs", type=int, default=4, help="worker processes for the baseline products")
+    parser.add_argument("--cache", default=os.path.join(tempfile.gettempdir(), "fherma_golden_cache.jsonl"),
+                        help="finished baseline products, one JSON line each (resumes an interrupted run)")
     args = parser.parse_args()
     ref = load_reference()
     header = {"generated_by": "tests/golden/make_golden.py",
@@ -177,7 +226,7 @@ def main():
     if args.only in (None, "reference"):
         (HERE / "reference_points.json").write_text(json.dumps({**header, "points": validate_points(ref)}, indent=1) + "\n")
     if args.only in (None, "baseline"):
-        (HERE / "baseline_cfg.json").write_text(json.dumps({**header, "points": baseline_points(ref, args.big)}, indent=1) + "\n")
+        (HERE / "baseline_cfg.json").write_text(json.dumps({**header, "points": baseline_points(args.big, args.jobs, args.cache)}, indent=1) + "\n")
 
 
 if __name__ == "__main__":

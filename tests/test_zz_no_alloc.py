@@ -10,6 +10,9 @@ The checks, through the C ABI:
 * two calls in a row match the existing negacyclic_run_device bit for bit, and the
   oracle too (integer product: tolerance 0);
 * the plan's own work-space binding is left as it was;
+* a call allocates nothing: the device's free memory is the same before and after a
+  synchronized call (once the first call has loaded the kernels);
+* device-side errors reach the plan's status word, which is clear after these calls;
 * a point too large for the array is refused with a message that says so.
 
 This file is collected last, so a run that stops at the first failure has run
@@ -55,6 +58,15 @@ def test_two_calls_match_run_device(n, limbs, seed, fpc, inputs, oracle, torch):
                 expect = oracle.kronecker(q, a, b)
                 assert np.array_equal(got.cpu().numpy().view(np.uint32), expect)
         assert fpc.pipeline_status() == 0
+        assert tables_only.status() == 0
+        # the property this entry point exists for: a call leaves the device's free memory as it was
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info()
+        tables_only.run_device_static(da.data_ptr(), db.data_ptr(), got.data_ptr(), stream)
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before
+        assert torch.equal(got, want)
         # the plan without a work space still has none: the static array was bound only for the call
         with pytest.raises(RuntimeError, match="no work space bound"):
             tables_only.run_device(da.data_ptr(), db.data_ptr(), got.data_ptr(), stream)
