@@ -34,7 +34,7 @@ EXPORTED = [
     "negacyclic_gemm_u8", "negacyclic_run_device_timed", "negacyclic_work_bytes", "negacyclic_bind_work",
     "negacyclic_pipeline_status", "negacyclic_run_begin", "negacyclic_run_finish",
     "negacyclic_prepare_host", "negacyclic_run_device_static", "negacyclic_plan_status",
-    "negacyclic_gemm_u8_withheld", "negacyclic_batch_status",
+    "negacyclic_gemm_u8_withheld", "negacyclic_batch_status", "negacyclic_host_touch",
     "negacyclic_batch_create", "negacyclic_batch_io", "negacyclic_batch_get_info", "negacyclic_batch_run_device",
     "negacyclic_batch_run", "negacyclic_batch_run_one", "negacyclic_batch_run_plain", "negacyclic_batch_free",
     "negacyclic_server_create", "negacyclic_server_open_session", "negacyclic_server_submit",
@@ -116,6 +116,7 @@ def library() -> ctypes.CDLL:
         lib.negacyclic_gemm_u8_withheld.argtypes = [p, p, p, u32, u32, u32, u32, ctypes.c_uint64, u32,
                                                     ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_double)]
         lib.negacyclic_batch_status.argtypes = [p, p]
+        lib.negacyclic_host_touch.argtypes = [p, p, ctypes.c_size_t]
         pp = ctypes.POINTER(p)
         lib.negacyclic_batch_create.argtypes = [ctypes.POINTER(PointSpec), u32, ctypes.POINTER(BatchOptions),
                                                 ctypes.POINTER(p)]

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -474,13 +475,20 @@ bool page_locked(const void* ptr) {
 }
 
 // Page-locked staging and the copy team of the host path, made on first use.
+// NEGACYCLIC_HOST_THREADS sets the team's size; by default it takes up to 6 of the host's cores.
+// Host memory bandwidth, shared with the copy engines and the caller's output fill, is the limit:
+// on a 16-core B200 host, fherma_run at N=65536, L=55 took 1.40-1.46 ms with 6 threads against
+// 1.52-1.62 with 8, 1.60-1.67 with 4 and 1.91 with 3 (0.65-0.77 ms at N=32768, L=28).
 void ensure_staging(negacyclic_plan& s) {
     const size_t words = size_t(s.host.n) * s.host.limbs;
     if (!s.stage_in) check(cudaHostAlloc(&s.stage_in, 2 * words * 4, cudaHostAllocWriteCombined), "cudaHostAlloc");
     if (!s.stage_out) check(cudaHostAlloc(&s.stage_out, words * 4, cudaHostAllocDefault), "cudaHostAlloc");
     if (!s.team) {
-        const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
-        s.team = std::make_unique<CopyTeam>(std::min(8u, hw / 2));
+        const unsigned hw = std::max(3u, std::thread::hardware_concurrency());
+        unsigned workers = std::min(6u, hw - 2);
+        if (const char* env = getenv("NEGACYCLIC_HOST_THREADS"))
+            workers = std::max(1u, std::min(64u, unsigned(std::strtoul(env, nullptr, 10))));
+        s.team = std::make_unique<HostTeam>(workers);
     }
 }
 
@@ -498,18 +506,25 @@ struct OutChunk {  // coefficients [first, first + count)
     uint32_t first, count;
 };
 
-bool transform_ordered_input(const negacyclic_plan& s);
+bool transform_ordered_input(const negacyclic_plan& s, bool packed_by_team);
 
 // Rows of at least 1 KB: chunks carry enough work that finer chunks near the ends (and one
 // transpose per output chunk) pay for their extra launches. Narrower rows keep equal chunks.
 bool wide_rows(const negacyclic_plan& s) { return s.host.limbs >= 256; }
+
+// Chunks of about `target` bytes out of `bytes`: a power of two in [2, min(most, limit)].
+uint32_t chunk_count(size_t bytes, size_t target, uint32_t most, uint32_t limit) {
+    uint32_t count = 2;
+    while (count * 2 <= std::min(most, limit) && bytes / (count * 2) >= target) count *= 2;
+    return std::max(1u, std::min(count, std::min(most, limit)));
+}
 
 // Chunk lists of a streamed host product (at most kMaxChunks each way).
 // In, transform-ordered: `parts` chunks per transform, the last transform cut finer, so that
 // little conversion is left once the link has delivered everything. In, coefficient-ordered:
 // equal coefficient ranges, the last one cut in four. Out: coefficient ranges growing from a
 // quarter of a chunk, so the copy-out starts soon after the last inverse NTT.
-void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vector<OutChunk>& out) {
+void stream_chunks(const negacyclic_plan& s, bool ordered, std::vector<InChunk>& in, std::vector<OutChunk>& out) {
     const HostPlan& h = s.host;
     const uint32_t split = h.split, n_sub = h.n_sub, per = h.n / s.chunks;
     constexpr uint32_t kMax = negacyclic_plan::kMaxChunks;
@@ -520,7 +535,7 @@ void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vect
         out.push_back(OutChunk{0, h.n});
         return;
     }
-    if (transform_ordered_input(s)) {
+    if (ordered) {
         const uint32_t parts = s.chunks / split;
         uint32_t tail = parts;  // power of two, spans of >= 256 rows, within the event budget
         while (tail * 2 <= 4 * parts && (split - 1) * parts + tail * 2 <= kMax && n_sub / (tail * 2) >= 256) tail *= 2;
@@ -528,26 +543,43 @@ void stream_chunks(const negacyclic_plan& s, std::vector<InChunk>& in, std::vect
             const uint32_t p = t + 1 == split ? tail : parts, span = n_sub / p;
             for (uint32_t k = 0; k < p; ++k) in.push_back(InChunk{t, k * span, span});
         }
-    } else {
+    } else if (wide_rows(s)) {
         const uint32_t quarter = per / 4;
-        const bool cut = wide_rows(s) && quarter / split >= 256 && s.chunks + 3 <= kMax;
+        const bool cut = quarter / split >= 256 && s.chunks + 3 <= kMax;
         for (uint32_t k = 0; k + 1 < s.chunks; ++k) in.push_back(InChunk{0, k * per, per});
         if (cut)
             for (uint32_t k = 0; k < 4; ++k) in.push_back(InChunk{0, (s.chunks - 1) * per + k * quarter, quarter});
         else
             in.push_back(InChunk{0, (s.chunks - 1) * per, per});
+    } else {
+        // narrow rows: about 2 MB of input per chunk (at least two chunks, at most s.chunks, and at
+        // least 256 positions of every transform each). Small copies carry fixed costs: 0.46 MB
+        // host-to-device copies ran at 23 GB/s against 55 for large ones (N=32768, L=28).
+        const uint32_t count = chunk_count(size_t(2) * h.n * h.limbs * 4, 2u << 20, s.chunks, n_sub / 256);
+        const uint32_t span = h.n / count;
+        for (uint32_t k = 0; k < count; ++k) in.push_back(InChunk{0, k * span, span});
     }
-    // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
-    uint32_t first = 0, size = (wide_rows(s) && per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
-    for (uint32_t k = 0; first < h.n; ++k) {
-        const uint32_t count = std::min(size, h.n - first);
-        out.push_back(OutChunk{first, count});
-        first += count;
-        if (k >= 1 && size < per) size *= 2;  // per/4, per/4, per/2, per, per, ...
+    if (wide_rows(s)) {  // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
+        uint32_t first = 0, size = (per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
+        for (uint32_t k = 0; first < h.n; ++k) {
+            const uint32_t count = std::min(size, h.n - first);
+            out.push_back(OutChunk{first, count});
+            first += count;
+            if (k >= 1 && size < per) size *= 2;  // per/4, per/4, per/2, per, per, ...
+        }
+        return;
     }
+    // narrow rows: about 1 MB of result per chunk, at least 256 coefficients each
+    const uint32_t count = chunk_count(size_t(h.n) * h.limbs * 4, 1u << 20, s.chunks, h.n / 256);
+    for (uint32_t k = 0; k < count; ++k) out.push_back(OutChunk{k * (h.n / count), h.n / count});
 }
 
-bool transform_ordered_input(const negacyclic_plan& s) {
+// Transform order needs rows gathered with a stride of s rows, by the copy engine as a 2-D copy
+// or by the host team while it packs pageable operands. Both pay only for rows of 1 KB or more:
+// a 2-D copy of 220-byte rows ran at a third of the link rate, and the team gathering 220-byte
+// rows packed at 20 GB/s against 55 GB/s for contiguous ranges (N=65536, L=55).
+bool transform_ordered_input(const negacyclic_plan& s, bool packed_by_team) {
+    (void)packed_by_team;
     return s.chunks > 1 && s.host.split > 1 && wide_rows(s);  // chunks >= split when chunked
 }
 
@@ -570,6 +602,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     const bool a_locked = page_locked(a), b_locked = page_locked(b);
     s.outputs_staged = !(c && page_locked(c));
     if (!a_locked || !b_locked || s.outputs_staged) ensure_staging(s);
+    if (s.pack_ticket) {  // a previous call that failed part-way may still be packing
+        s.team->wait(s.pack_ticket);
+        s.pack_ticket = 0;
+    }
     check(cudaMemsetAsync(s.status, 0, 4, st), "memset");
     const uint32_t* src[2] = {a, b};
     const bool locked[2] = {a_locked, b_locked};
@@ -578,20 +614,63 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     // every chunk is converted, stages them
     std::vector<InChunk> in;
     std::vector<OutChunk> out;
-    stream_chunks(s, in, out);
-    if (transform_ordered_input(s)) {
+    const bool ordered = transform_ordered_input(s, !a_locked && !b_locked);
+    stream_chunks(s, ordered, in, out);
+    uint32_t pieces[negacyclic_plan::kMaxChunks] = {};  // pack pieces per input chunk
+    if (!a_locked || !b_locked) {
+        // One pack job over pieces of about kPieceBytes of the pageable operands, claimed in chunk
+        // order from a shared counter (a descheduled worker holds up at most the piece it has);
+        // packed[k] counts chunk k's pieces done, and the loops below hand chunk k to the copy
+        // engine as soon as all of them are, while later chunks are still being packed.
+        constexpr size_t kPieceBytes = 256 << 10;
+        const uint32_t per_piece = uint32_t(std::max<size_t>(1, kPieceBytes / row));  // rows per piece
+        const uint32_t operands = (a_locked ? 0u : 1u) + (b_locked ? 0u : 1u);
+        std::vector<uint32_t> first_piece(in.size() + 1, 0);
+        for (uint32_t k = 0; k < in.size(); ++k) {
+            pieces[k] = operands * ((in[k].span + per_piece - 1) / per_piece);
+            first_piece[k + 1] = first_piece[k] + pieces[k];
+            s.packed[k].store(0, std::memory_order_relaxed);
+        }
+        s.next_piece.store(0, std::memory_order_relaxed);
+        uint32_t* stage = s.stage_in;
+        const uint32_t n = h.n, limbs = h.limbs, total = first_piece.back();
+        std::atomic<uint32_t>* packed = s.packed;
+        std::atomic<uint32_t>* next = &s.next_piece;
+        s.pack_ticket = s.team->post([=](unsigned, unsigned) {
+            uint32_t k = 0;
+            for (uint32_t piece = next->fetch_add(1, std::memory_order_relaxed); piece < total;
+                 piece = next->fetch_add(1, std::memory_order_relaxed)) {
+                while (piece >= first_piece[k + 1]) ++k;
+                const InChunk ch = in[k];
+                const uint32_t local = piece - first_piece[k], per_op = pieces[k] / operands;
+                const int op = operands == 2 ? int(local / per_op) : (a_locked ? 1 : 0);
+                const size_t first = size_t(local % per_op) * per_piece;
+                const size_t last = std::min<size_t>(ch.span, first + per_piece);
+                if (ordered) {  // gather rows s*j + t to their split-major places t*N' + j
+                    const size_t host_row0 = size_t(split) * ch.j0 + ch.t, buf_row0 = size_t(ch.t) * n_sub + ch.j0;
+                    const uint32_t* from = src[op] + host_row0 * limbs;
+                    uint32_t* to = stage + (op * size_t(n) + buf_row0) * limbs;
+                    for (size_t j = first; j < last; ++j) std::memcpy(to + j * limbs, from + j * split * limbs, row);
+                } else {  // a contiguous coefficient range
+                    const size_t at = (size_t(ch.j0) + first) * limbs;
+                    std::memcpy(stage + op * size_t(n) * limbs + at, src[op] + at, (last - first) * row);
+                }
+                packed[k].fetch_add(1, std::memory_order_release);
+            }
+        });
+    }
+    if (ordered) {
         const bool direct = s.padded_limbs == h.limbs;
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
         for (uint32_t k = 0; k < in.size(); ++k) {
             const InChunk ch = in[k];
             const size_t host_row0 = size_t(split) * ch.j0 + ch.t, buf_row0 = size_t(ch.t) * n_sub + ch.j0;
+            spin_until(s.packed[k], pieces[k]);
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + host_row0 * h.limbs;
                 size_t pitch = split * row;
-                if (!locked[op]) {  // gather the chunk's rows into stage_in at their split-major places
-                    uint32_t* gathered = s.stage_in + (op * size_t(h.n) + buf_row0) * h.limbs;
-                    s.team->copy_rows(gathered, row, from, pitch, row, ch.span);
-                    from = gathered;
+                if (!locked[op]) {  // packed into stage_in at the rows' split-major places
+                    from = s.stage_in + (op * size_t(h.n) + buf_row0) * h.limbs;
                     pitch = row;
                 }
                 copy_rows_async(staged + (op * size_t(h.n) + buf_row0) * h.limbs, row, from, pitch, row, ch.span,
@@ -610,12 +689,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
         for (uint32_t k = 0; k < in.size(); ++k) {
             const size_t first = in[k].j0, count = in[k].span, bytes = count * row;  // coefficient range
+            spin_until(s.packed[k], pieces[k]);
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + first * h.limbs;
-                if (!locked[op]) {
-                    s.team->copy(s.stage_in + op * words + first * h.limbs, from, bytes);
-                    from = s.stage_in + op * words + first * h.limbs;
-                }
+                if (!locked[op]) from = s.stage_in + op * words + first * h.limbs;  // packed by the team
                 check(cudaMemcpyAsync(staged + op * words + first * h.limbs, from, bytes, cudaMemcpyHostToDevice,
                                       s.copy_in),
                       "copy in");
@@ -658,18 +735,39 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     check(cudaGetLastError(), "product kernels");
 }
 
-// Waits for a host product; copies staged output chunks into c as they land.
+// Waits for a host product; the team copies each staged output chunk into c as soon as its
+// copy-out has completed.
 int host_finish(negacyclic_plan& s, uint32_t* c) {
     const HostPlan& h = s.host;
+    if (s.pack_ticket) {  // every chunk was issued only after it was packed: the job is done
+        s.team->wait(s.pack_ticket);
+        s.pack_ticket = 0;
+    }
     if (s.outputs_staged) {
         std::vector<InChunk> in;
         std::vector<OutChunk> out;
-        stream_chunks(s, in, out);
+        stream_chunks(s, false, in, out);  // the output chunks do not depend on the input order
+        // one unpack job per output chunk, posted as soon as its copy-out has completed: the
+        // workers copy their slices of it into c while later chunks are still on the way (and
+        // sleep, instead of spinning, while the device computes)
+        const uint32_t limbs = h.limbs;
+        const uint32_t* stage = s.stage_out;
+        std::string failed;
+        uint64_t ticket = 0;
         for (uint32_t k = 0; k < out.size(); ++k) {
-            check(cudaEventSynchronize(s.copied_out[k]), "copy c");
-            const size_t first = out[k].first;
-            s.team->copy(c + first * h.limbs, s.stage_out + first * h.limbs, size_t(out[k].count) * h.limbs * 4);
+            const cudaError_t e = cudaEventSynchronize(s.copied_out[k]);
+            if (e != cudaSuccess) {
+                failed = cudaGetErrorString(e);
+                break;
+            }
+            const size_t words = size_t(out[k].count) * limbs, at = size_t(out[k].first) * limbs;
+            ticket = s.team->post([=](unsigned w, unsigned workers) {
+                const size_t b = HostTeam::slice_begin(words, w, workers), e = HostTeam::slice_begin(words, w + 1, workers);
+                if (e > b) std::memcpy(c + at + b, stage + at + b, (e - b) * 4);
+            });
         }
+        if (ticket) s.team->wait(ticket);
+        if (!failed.empty()) return fail(NEGACYCLIC_ECUDA, "copy c: " + failed);
     }
     check(cudaStreamSynchronize(s.copy_out), "product");
     check(cudaStreamSynchronize(s.stream), "product");
@@ -738,6 +836,17 @@ int negacyclic_run_finish(negacyclic_plan* s, uint32_t* c) {
     } catch (const CudaError& e) {
         return cuda_failure(e);
     }
+}
+
+int negacyclic_host_touch(negacyclic_plan* s, void* ptr, size_t bytes) {
+    if (!s || (!ptr && bytes)) return fail(NEGACYCLIC_EINVAL, "NULL argument");
+    try {
+        ensure_staging(*s);
+    } catch (const CudaError& e) {
+        return cuda_failure(e);
+    }
+    s->team->touch(ptr, bytes);
+    return NEGACYCLIC_OK;
 }
 
 void negacyclic_free(negacyclic_plan* plan) { delete plan; }

@@ -11,6 +11,7 @@
 #include "host_io.h"
 #include "kernels.cuh"
 
+#include <atomic>
 #include <memory>
 
 // The C ABI's opaque plan (include/negacyclic.h).
@@ -43,7 +44,10 @@ struct negacyclic_plan {
     // host path with pageable arrays: page-locked staging and a copy team (made on first use)
     uint32_t* stage_in = nullptr;   // [2][N][L], write-combined
     uint32_t* stage_out = nullptr;  // [N][L]
-    std::unique_ptr<negacyclic::CopyTeam> team;
+    std::unique_ptr<negacyclic::HostTeam> team;
+    std::atomic<uint32_t> packed[kMaxChunks] = {};  // pieces of input chunk k packed
+    std::atomic<uint32_t> next_piece{0};            // next unclaimed piece of the running pack job
+    uint64_t pack_ticket = 0;                       // the running call's pack job (0: none)
     bool outputs_staged = false;    // the running host product copies c through stage_out
     size_t device_bytes = 0, table_bytes = 0;
     negacyclic::TensorGemmPlan convert_gemm, crt_gemm;

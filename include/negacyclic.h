@@ -117,11 +117,24 @@ int negacyclic_prepare_host(negacyclic_plan* plan);
 /*
  * negacyclic_run in two halves, so that a caller can do host work (such as
  * allocating the output array) while the device computes: begin enqueues
- * everything with the result staged in page-locked memory; finish waits and
- * copies it into c. a and b must stay valid until finish returns.
+ * everything with the result staged in page-locked memory (pageable inputs are
+ * packed into staging by the plan's host threads, each chunk handed to the copy
+ * engine as soon as it is packed); finish waits and has the host threads copy
+ * each output chunk into c as it lands. a and b must stay valid until finish
+ * returns.
  */
 int negacyclic_run_begin(negacyclic_plan* plan, const uint32_t* a, const uint32_t* b);
 int negacyclic_run_finish(negacyclic_plan* plan, uint32_t* c);
+
+/*
+ * Writes zeros over host memory [ptr, ptr + bytes) with the plan's host threads, so
+ * that the first touch of a freshly allocated output array (page faults and the
+ * kernel's zeroing, about 0.35 ms per MB on one core) is paid by all of them at
+ * once. For callers that must allocate a new output array per product, as the
+ * reference's fherma_run does (src/solve.cu:611); call it between run_begin and
+ * run_finish, while the device computes. Blocking.
+ */
+int negacyclic_host_touch(negacyclic_plan* plan, void* ptr, size_t bytes);
 
 /*
  * Device-resident product: d_a, d_b, d_c are device arrays of n*limbs words on

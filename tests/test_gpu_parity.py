@@ -195,6 +195,30 @@ def test_streamed_host_path_with_sixteen_transforms(limbs, fpc, inputs, oracle, 
         assert np.array_equal(oracle.schoolbook_at(q, a, b, i)[0], host[i]), i
 
 
+@pytest.mark.parametrize("n,limbs", [(65536, 55), (32768, 28), (8192, 300)])
+def test_host_path_locking_combinations(n, limbs, fpc, inputs, torch):
+    """The host path with page-locked and pageable arrays in every combination: pageable inputs
+    are packed by the host team (transform order when the ring is split), page-locked ones go
+    straight to the copy engine (coefficient order for rows under 1 KB); pageable outputs are
+    unpacked by the team as chunks land. All must equal the device-resident product."""
+    q, a, b = inputs.instance(n, limbs, 4242, 0)
+    with fpc.Plan(n, 32 * limbs, limbs, q) as plan:
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(b.view(np.int32)).cuda()
+        dc = torch.empty_like(da)
+        plan.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        want = dc.cpu().numpy().view(np.uint32)
+        pin = lambda x: torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)  # noqa: E731
+        pa, pb, pc = pin(a), pin(b), pin(np.zeros_like(a))
+        for x, y, out in [(a, b, None), (pa, pb, pc), (pa, b, None), (a, pb, pc), (pa, pb, None), (a, b, pc)]:
+            got = plan.run(x, y, out=out if out is not None else np.zeros_like(a))
+            assert np.array_equal(got, want)
+            if out is not None:
+                out[:] = 0
+        assert plan.status() == 0
+
+
 # ---------------------------------------------------------------- full-size configurations
 
 def big_points():
