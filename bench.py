@@ -672,6 +672,9 @@ def run_batch(args):
     log(f"host arrays: batched {host_batched_ms:.1f} ms, plain {host_plain_ms:.1f} ms")
     ops = sum(2.0 * (2 * n) * (4 * l) * (4 * batch.info(i)["primes"]) + 2.0 * n * (4 * batch.info(i)["primes"]) *
               (4 * (l + 5)) for i, (n, l, *_r) in enumerate(instances))
+    infos = [batch.info(i) for i in range(len(instances))]
+    batch.close()
+    small = small_half(fpc, torch, instances, infos, args, cudart)
     line = {"metric": f"products/s, {len(instances)} uneven products (N in 4096..65536, L log-uniform 32..1747)",
             "value": len(instances) / (batched_ms / 1000), "unit": "products/s", "mode": "batched graph",
             "plain_value": len(instances) / (plain_ms / 1000), "batched_over_plain": plain_ms / batched_ms,
@@ -680,10 +683,54 @@ def run_batch(args):
                          "plain_products_per_s": len(instances) / (host_plain_ms / 1000),
                          "batched_over_plain": host_plain_ms / host_batched_ms,
                          "bytes_per_batch": int(sum(3 * a.nbytes for _, _, _, a, _ in instances))},
-            "lanes": args.lanes or 1, "tuned": bool(args.tune), "setup_s": setup_s,
+            "lanes": args.lanes or "two phases (concurrent small instances on up to 4 lanes, then large ones alone)",
+            "concurrent_phase": small,
+            "tuned": bool(args.tune), "setup_s": setup_s,
             "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seed 100)"}
     print(json.dumps(line), flush=True)
+
+
+def small_half(fpc, torch, instances, infos, args, cudart) -> dict:
+    """The batch's concurrent phase alone (the instances under about 1 ms of device time): one
+    graph launch of just those instances against the plain per-call loop over the same ones."""
+    chosen = [i for i, info in enumerate(infos) if info["phase"] == 0]
+    if not chosen:
+        return {"instances": 0}
+    subset = [instances[i] for i in chosen]
+    batch = fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in subset], lanes=args.lanes, tune=args.tune,
+                      tune_cache=args.tune_cache)
+    for j, (n, l, q, a, b) in enumerate(subset):
+        da, db, _ = batch.io(j)
+        cudart.cudaMemcpy(da, a.ctypes.data, a.nbytes, 1)
+        cudart.cudaMemcpy(db, b.ctypes.data, b.nbytes, 1)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(max(3, args.warmup)):
+        batch.run_device(sptr)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        batch.run_device(sptr)
+    stop.record(stream)
+    stop.synchronize()
+    batched_ms = start.elapsed_time(stop) / args.steps
+    if batch.status().any():
+        raise RuntimeError("concurrent phase: a status word is set")
+    plain_ms = 0.0
+    for _ in range(max(1, args.steps // 2)):
+        start.record(stream)
+        for j in range(len(subset)):
+            batch.run_one(j, sptr)
+            stream.synchronize()
+        stop.record(stream)
+        stop.synchronize()
+        plain_ms += start.elapsed_time(stop) / max(1, args.steps // 2)
+    lanes = sorted({batch.info(j)["lane"] for j in range(len(subset))})
     batch.close()
+    return {"instances": len(subset), "shapes": [[n, l] for n, l, *_r in subset], "lanes": len(lanes),
+            "batched_ms": batched_ms, "plain_ms": plain_ms, "batched_products_per_s": len(subset) / (batched_ms / 1000),
+            "plain_products_per_s": len(subset) / (plain_ms / 1000), "batched_over_plain": plain_ms / batched_ms}
 
 
 def run_serve(args):
@@ -697,7 +744,7 @@ def run_serve(args):
     rng = np.random.Generator(np.random.PCG64(200))
     max_limbs = args.serve_max_limbs
     sessions = []
-    server = fpc.Server(hbm_budget=int(args.budget_gb * (1 << 30)), slots=args.slots)
+    server = fpc.Server(hbm_budget=int(args.budget_gb * (1 << 30)), slots=args.slots, max_queue=args.max_queue)
     for sidx in range(8):
         limbs = int(np.floor(np.exp(rng.uniform(np.log(32), np.log(max_limbs + 1)))))
         q = inputs.random_modulus(limbs, 200 + sidx)
@@ -736,10 +783,10 @@ def run_serve(args):
 
     runs = []
     for rate in [float(x) for x in args.rates.split(",")]:
-        # offered load above capacity queues up: a shorter arrival window keeps the drain bounded
-        duration = args.duration if rate <= 400 else args.duration * 400 / rate
+        duration = args.duration  # the same arrival window at every rate; overload is shed at submit
         schedule = schedule_for(rate, duration)
-        ids, out_counter = [], {}
+        ids, out_counter, refused = [], {}, 0
+        before = server.stats()
         start = time.perf_counter()
         for when, s_index, n, k in schedule:
             delay = when - (time.perf_counter() - start)
@@ -750,13 +797,20 @@ def run_serve(args):
             slot = out_counter.get((sid, n), 0)
             out_counter[(sid, n)] = slot + 1
             a, b = pool[n][k]
-            ids.append(server.submit(sid, a, b, out=ring[slot % len(ring)]))
+            rid = server.submit(sid, a, b, out=ring[slot % len(ring)])
+            if rid is None:
+                refused += 1
+            else:
+                ids.append(rid)
         latencies = np.array([server.wait(rid)[1] for rid in ids])
         elapsed = time.perf_counter() - start
-        runs.append({"offered_rate": rate, "arrival_window_s": round(duration, 3), "requests": len(ids),
-                     "products_per_s": len(ids) / elapsed, "p50_ms": float(np.percentile(latencies, 50)),
-                     "p99_ms": float(np.percentile(latencies, 99)), "mean_ms": float(latencies.mean()),
-                     "elapsed_s": round(elapsed, 3)})
+        after = server.stats()
+        runs.append({"offered_rate": rate, "arrival_window_s": round(duration, 3), "offered": len(schedule),
+                     "completed": len(ids), "rejected": refused,
+                     "rejected_by_server": int(after["rejected"] - before["rejected"]),
+                     "max_queue_depth": int(after["max_queued"]), "products_per_s": len(ids) / elapsed,
+                     "p50_ms": float(np.percentile(latencies, 50)), "p99_ms": float(np.percentile(latencies, 99)),
+                     "mean_ms": float(latencies.mean()), "elapsed_s": round(elapsed, 3)})
         log(f"rate {rate:g}: {runs[-1]}")
     stats = server.stats()
     server.close()
@@ -784,6 +838,7 @@ def run_serve(args):
             "value": best, "unit": "products/s", "mode": "serving (continuous batching)", "runs": runs,
             "plain_per_call_products_per_s": plain_value, "plain_requests": len(mix),
             "served_over_plain": best / plain_value, "slots": args.slots, "hbm_budget_gb": args.budget_gb,
+            "max_queue": args.max_queue,
             "session_limbs": [limbs for _, limbs, _, _ in sessions], "failed": stats["failed"],
             "warmup": {"requests": len(warm), "seconds": round(warm_s, 3)},
             "data": "synthetic (seed 200)"}
@@ -822,12 +877,14 @@ def main():
                         help="plain: the benchmark line; batch / serve: the batched and serving forms; "
                              "cpu-calibrate: one full-size CPU product against the bounded sample")
     parser.add_argument("--count", type=int, default=64, help="batch: number of uneven products")
-    parser.add_argument("--lanes", type=int, default=0, help="batch: compute lanes (0 = 1)")
+    parser.add_argument("--lanes", type=int, default=0,
+                        help="batch: compute lanes (0 = two phases: small instances concurrently, then large ones)")
     parser.add_argument("--tune", action="store_true", help="batch: run the autotuner for uncached shapes")
     parser.add_argument("--tune-cache", default=None, help="batch: autotuner cache file")
     parser.add_argument("--rates", default="200,1000,5000", help="serve: Poisson arrival rates (requests/s)")
-    parser.add_argument("--duration", type=float, default=10.0,
-                        help="serve: seconds of arrivals (scaled down above 400 requests/s)")
+    parser.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals at each rate")
+    parser.add_argument("--max-queue", type=int, default=64,
+                        help="serve: requests waiting for admission beyond which submits are refused")
     parser.add_argument("--plain-requests", type=int, default=200, help="serve: requests of the plain comparison")
     parser.add_argument("--slots", type=int, default=4, help="serve: concurrent requests")
     parser.add_argument("--budget-gb", type=float, default=60.0, help="serve: HBM budget (GiB)")

@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY = os.path.join(HERE, "libnegacyclic.so")
 SHIM_LIBRARY = os.path.join(HERE, "libfherma_negacyclic.so")
 
-OK, EINVAL, ENOFIELDS, ESIZE, ECUDA, ENOMEM, ENODEV = range(7)
+OK, EINVAL, ENOFIELDS, ESIZE, ECUDA, ENOMEM, ENODEV, EBUSY = range(8)
 GEMM_AUTO, GEMM_SIMT, GEMM_TENSOR, GEMM_TENSOR_SINGLE = 0, 1, 2, 3
 STATUS_REDUCE, STATUS_GEMM_MASK = 0x1, 0x1ffff00
 
@@ -67,19 +67,19 @@ class BatchOptions(ctypes.Structure):
 
 class BatchInstance(ctypes.Structure):
     _fields_ = [("plan", Info), ("lane", ctypes.c_uint32), ("requested_gemm", ctypes.c_uint32),
-                ("tuned_ms", ctypes.c_double)]
+                ("tuned_ms", ctypes.c_double), ("phase", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_uint64), ("slots", ctypes.c_uint32), ("device", ctypes.c_int32),
-                ("reserved", ctypes.c_uint32 * 4)]
+                ("max_queue", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("queued", ctypes.c_uint64),
                 ("resident_bytes", ctypes.c_uint64), ("in_flight_bytes", ctypes.c_uint64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
-                ("products_per_s", ctypes.c_double)]
+                ("products_per_s", ctypes.c_double), ("rejected", ctypes.c_uint64), ("max_queued", ctypes.c_uint64)]
 
 
 _lib = None
@@ -307,7 +307,7 @@ class Batch:
         inst = BatchInstance()
         _check(library().negacyclic_batch_get_info(self._handle, index, ctypes.byref(inst)), "negacyclic_batch_get_info")
         out = {name: getattr(inst.plan, name) for name, _ in Info._fields_}
-        out.update(lane=inst.lane, requested_gemm=inst.requested_gemm, tuned_ms=inst.tuned_ms)
+        out.update(lane=inst.lane, requested_gemm=inst.requested_gemm, tuned_ms=inst.tuned_ms, phase=inst.phase)
         return out
 
     def run_device(self, stream: int = 0):
@@ -349,8 +349,8 @@ class Batch:
 class Server:
     """Request loop with continuous batching (negacyclic_server_*)."""
 
-    def __init__(self, hbm_budget: int = 0, slots: int = 0, device: int = -1):
-        opts = ServerOptions(hbm_budget, slots, device)
+    def __init__(self, hbm_budget: int = 0, slots: int = 0, device: int = -1, max_queue: int = 0):
+        opts = ServerOptions(hbm_budget, slots, device, max_queue)
         handle = ctypes.c_void_p()
         _check(library().negacyclic_server_create(ctypes.byref(opts), ctypes.byref(handle)), "negacyclic_server_create")
         self._handle = handle
@@ -366,11 +366,15 @@ class Server:
         return session.value
 
     def submit(self, session: int, a, b, out=None) -> int:
+        """Request id, or None when the server's queue is full (the request was refused)."""
         a, b = _u32(a), _u32(b)
         c = np.empty_like(a) if out is None else out
         rid = ctypes.c_uint64()
-        _check(library().negacyclic_server_submit(self._handle, session, a.shape[0], a.ctypes.data, b.ctypes.data,
-                                                  c.ctypes.data, ctypes.byref(rid)), "negacyclic_server_submit")
+        status = library().negacyclic_server_submit(self._handle, session, a.shape[0], a.ctypes.data, b.ctypes.data,
+                                                    c.ctypes.data, ctypes.byref(rid))
+        if status == EBUSY:
+            return None
+        _check(status, "negacyclic_server_submit")
         self._keep[rid.value] = (a, b, c)
         return rid.value
 

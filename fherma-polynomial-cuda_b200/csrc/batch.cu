@@ -8,10 +8,17 @@
 //     length N' = N/s and the prime set) and the GEMM kernel (CTA-pair 256x256
 //     tiles, single-CTA 128x256 tiles, or the SIMT kernel) by timing each
 //     candidate on the device; results are cached in a text file;
-//   * instances are assigned longest-first to `lanes` compute streams (one by
-//     default: a large product fills the GPU by itself, and a single lane may use
-//     the CTA-pair GEMM kernel); each lane owns one work arena (sized for its
-//     largest instance) that its instances use one after another;
+//   * by default the batch runs in two phases. Small instances (a tuned or estimated
+//     device time under kSmallMs) run first, concurrently, assigned longest-first to
+//     kSmallLanes compute streams with single-CTA tensor GEMMs: a small product
+//     leaves most of the GPU idle between its short kernels, and other instances'
+//     kernels fill those gaps. The large instances then run one after another on
+//     lane 0 with the CTA-pair GEMM, which fills the GPU by itself and never shares
+//     it with another kernel (several cluster kernels resident at once stalled);
+//   * `lanes` > 0 instead assigns every instance longest-first to that many lanes
+//     (single-CTA GEMMs when more than one);
+//   * each lane owns one work arena (sized for its largest instance, lane 0's for the
+//     large phase too) that its instances use one after another;
 //   * the whole batch — every lane's chain of products — is captured once into a
 //     CUDA graph, so a batch run is a single cudaGraphLaunch;
 //   * with host arrays, operand copies run on a copy-in stream and result copies
@@ -147,12 +154,17 @@ double estimate_ms(const negacyclic_plan& plan) {
 
 }  // namespace
 
+// Automatic lanes: instances under kSmallMs of device time share the GPU on kSmallLanes streams.
+constexpr double kSmallMs = 1.0;
+constexpr uint32_t kSmallLanes = 4;
+
 struct negacyclic_batch {
     int device = 0;
     std::vector<std::unique_ptr<negacyclic_plan>> plans;
     std::vector<TuneChoice> choices;
     std::vector<uint32_t> lane_of;
-    std::vector<std::vector<uint32_t>> lane_order;
+    std::vector<std::vector<uint32_t>> lane_order;  // the concurrent phase, per lane
+    std::vector<uint32_t> large;                    // the sequential phase (lane 0), in order
     std::vector<cudaStream_t> lanes;
     std::vector<void*> arenas;
     void* io = nullptr;
@@ -160,7 +172,7 @@ struct negacyclic_batch {
     std::vector<size_t> io_offset;  // a, then b, then c per instance
     cudaStream_t capture = nullptr, copy_in = nullptr, copy_out = nullptr;
     std::vector<cudaEvent_t> copied_in, computed;  // per instance, host-array runs
-    cudaEvent_t fork = nullptr;
+    cudaEvent_t fork = nullptr, phase = nullptr;
     std::vector<cudaEvent_t> joins;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -178,6 +190,7 @@ struct negacyclic_batch {
         if (copy_in) cudaStreamDestroy(copy_in);
         if (copy_out) cudaStreamDestroy(copy_out);
         if (fork) cudaEventDestroy(fork);
+        if (phase) cudaEventDestroy(phase);
         for (cudaStream_t s : lanes) cudaStreamDestroy(s);
         if (capture) cudaStreamDestroy(capture);
         for (void* a : arenas) cudaFree(a);
@@ -248,37 +261,47 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
             save_cache(cache_path, cache);
         }
 
-        // 2. longest-first assignment to lanes
-        const uint32_t lanes = o.lanes ? std::min(o.lanes, count) : 1u;
-        // Products on several lanes run concurrently: they use the single-CTA tensor-core kernel,
-        // because concurrent launches of the CTA-pair (cluster) kernel from several streams stalled.
-        if (lanes > 1)
-            for (auto& plan : b->plans) plan->gemm_pairs_allowed = false;
+        // 2. lanes: longest-first assignment of the concurrent phase's instances
         std::vector<double> cost(count);
         for (uint32_t i = 0; i < count; ++i)
             cost[i] = b->choices[i].ms > 0 ? b->choices[i].ms : estimate_ms(*b->plans[i]);
         std::vector<uint32_t> order(count);
         std::iota(order.begin(), order.end(), 0u);
         std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
+        std::vector<uint32_t> concurrent;
+        if (o.lanes) {
+            concurrent = order;  // every instance shares the lanes the caller asked for
+        } else {
+            for (uint32_t i : order) (cost[i] < kSmallMs ? concurrent : b->large).push_back(i);
+        }
+        const uint32_t lanes = o.lanes ? std::min(o.lanes, count)
+                                       : std::max(1u, std::min<uint32_t>(kSmallLanes, uint32_t(concurrent.size())));
+        // Products on several lanes run concurrently: they use the single-CTA tensor-core kernel,
+        // because concurrent launches of the CTA-pair (cluster) kernel from several streams stalled.
+        if (lanes > 1)
+            for (uint32_t i : concurrent) b->plans[i]->gemm_pairs_allowed = false;
         std::vector<double> load(lanes, 0.0);
         b->lane_of.assign(count, 0);
         b->lane_order.assign(lanes, {});
-        for (uint32_t i : order) {
+        for (uint32_t i : concurrent) {
             const uint32_t lane = uint32_t(std::min_element(load.begin(), load.end()) - load.begin());
             load[lane] += cost[i];
             b->lane_of[i] = lane;
             b->lane_order[lane].push_back(i);
         }
 
-        // 3. device memory: one work arena per lane, one I/O arena for every instance
+        // 3. device memory: one work arena per lane (lane 0's also serves the sequential phase),
+        // one I/O arena for every instance
         b->lanes.resize(lanes);
         b->arenas.assign(lanes, nullptr);
         for (uint32_t lane = 0; lane < lanes; ++lane) {
             check(cudaStreamCreateWithFlags(&b->lanes[lane], cudaStreamNonBlocking), "cudaStreamCreate");
+            std::vector<uint32_t> users = b->lane_order[lane];
+            if (lane == 0) users.insert(users.end(), b->large.begin(), b->large.end());
             size_t need = 256;
-            for (uint32_t i : b->lane_order[lane]) need = std::max(need, b->plans[i]->work_bytes);
+            for (uint32_t i : users) need = std::max(need, b->plans[i]->work_bytes);
             check(cudaMalloc(&b->arenas[lane], need), "cudaMalloc");
-            for (uint32_t i : b->lane_order[lane]) {
+            for (uint32_t i : users) {
                 const std::string why = bind_work(*b->plans[i], b->arenas[lane]);
                 if (!why.empty()) return fail(NEGACYCLIC_EINVAL, why);
             }
@@ -307,6 +330,7 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
         // 4. capture every lane's chain of products into one graph
         check(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&b->phase, cudaEventDisableTiming), "cudaEventCreate");
         b->joins.resize(lanes);
         for (auto& e : b->joins) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         check(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -319,6 +343,15 @@ int negacyclic_batch_create(const negacyclic_point* points, uint32_t count, cons
                     enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), b->lanes[lane]);
                 check(cudaEventRecord(b->joins[lane], b->lanes[lane]), "cudaEventRecord");
                 check(cudaStreamWaitEvent(b->capture, b->joins[lane], 0), "cudaStreamWaitEvent");
+            }
+            // the sequential phase, on lane 0 once every lane has finished
+            if (!b->large.empty()) {
+                check(cudaEventRecord(b->phase, b->capture), "cudaEventRecord");
+                check(cudaStreamWaitEvent(b->lanes[0], b->phase, 0), "cudaStreamWaitEvent");
+                for (uint32_t i : b->large)
+                    enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), b->lanes[0]);
+                check(cudaEventRecord(b->joins[0], b->lanes[0]), "cudaEventRecord");
+                check(cudaStreamWaitEvent(b->capture, b->joins[0], 0), "cudaStreamWaitEvent");
             }
         } catch (...) {
             cudaGraph_t abandoned = nullptr;
@@ -352,6 +385,7 @@ int negacyclic_batch_get_info(const negacyclic_batch* b, uint32_t index, negacyc
     *info = negacyclic_batch_instance{};
     negacyclic_get_info(b->plans[index].get(), &info->plan);
     info->lane = b->lane_of[index];
+    info->phase = std::find(b->large.begin(), b->large.end(), index) != b->large.end() ? 1u : 0u;
     info->tuned_ms = b->choices[index].ms;
     info->requested_gemm = b->choices[index].gemm;
     return NEGACYCLIC_OK;
@@ -381,21 +415,32 @@ int negacyclic_batch_run(negacyclic_batch* b, const uint32_t* const* a, const ui
     if (!b || !a || !bb || !c) return fail(NEGACYCLIC_EINVAL, "NULL argument");
     DeviceGuard guard(b->device);
     try {
-        // issue order: round-robin over the lanes' sequences, so every lane gets work early
+        // issue order: round-robin over the concurrent lanes' sequences, so every lane gets work
+        // early, then the sequential phase
         std::vector<uint32_t> order;
         std::vector<size_t> next(b->lanes.size(), 0);
-        while (order.size() < b->plans.size())
+        size_t concurrent = 0;
+        for (const auto& lane : b->lane_order) concurrent += lane.size();
+        while (order.size() < concurrent)
             for (uint32_t lane = 0; lane < b->lanes.size(); ++lane)
                 if (next[lane] < b->lane_order[lane].size()) order.push_back(b->lane_order[lane][next[lane]++]);
+        order.insert(order.end(), b->large.begin(), b->large.end());
         // copy-in -> compute (the instance's lane) -> copy-out, linked by events; every lane's first
-        // product waits for a copy-in event recorded after the status words are cleared
+        // product waits for a copy-in event recorded after the status words are cleared; the first
+        // product of the sequential phase also waits for every lane's last concurrent product
         check(cudaMemsetAsync(b->status, 0, b->plans.size() * sizeof(uint32_t), b->copy_in), "cudaMemsetAsync");
-        for (uint32_t i : order) {
+        for (size_t at = 0; at < order.size(); ++at) {
+            const uint32_t i = order[at];
             const size_t bytes = b->words(i) * 4;
             check(cudaMemcpyAsync(b->slot(i, 0), a[i], bytes, cudaMemcpyHostToDevice, b->copy_in), "copy a");
             check(cudaMemcpyAsync(b->slot(i, 1), bb[i], bytes, cudaMemcpyHostToDevice, b->copy_in), "copy b");
             check(cudaEventRecord(b->copied_in[i], b->copy_in), "cudaEventRecord");
             cudaStream_t lane = b->lanes[b->lane_of[i]];
+            if (at == concurrent && concurrent > 0)
+                for (uint32_t other = 1; other < b->lanes.size(); ++other) {
+                    check(cudaEventRecord(b->joins[other], b->lanes[other]), "cudaEventRecord");
+                    check(cudaStreamWaitEvent(lane, b->joins[other], 0), "cudaStreamWaitEvent");
+                }
             check(cudaStreamWaitEvent(lane, b->copied_in[i], 0), "cudaStreamWaitEvent");
             enqueue_device_product(*b->plans[i], b->slot(i, 0), b->slot(i, 1), b->slot(i, 2), lane);
             check(cudaEventRecord(b->computed[i], lane), "cudaEventRecord");

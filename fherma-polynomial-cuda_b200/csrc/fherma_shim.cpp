@@ -16,6 +16,8 @@
 #endif
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 
 #include <condition_variable>
 #include <cstdint>
@@ -34,8 +36,11 @@ namespace {
 // calling thread packs the operands and launches the product. std::vector value-initialises
 // its elements on one core, and fresh pages fault one 4 KB page at a time: 156-160 ms for the
 // 458 MB result of N=65536, L=1747 on a B200 host. Reserving first and asking for transparent
-// huge pages over the reserved range before the zero-fill cuts that to 54 ms (0.45 ms instead
-// of 0.7-5.3 ms at N=65536, L=55), all of it overlapped with the transfer and the product.
+// huge pages over the reserved range (when it spans at least kHugeBytes) cuts that to 54 ms.
+// After the fill the thread keeps spinning until the call is over (release(), or kActiveFor):
+// on a B200 box's virtual host, copy threads writing lines that this thread had just zeroed,
+// once it slept, took ~300 us for the last 1.8 MB output chunk instead of ~35, and the device's
+// reads of host memory also slowed while host cores idled.
 class OutputBuilder {
 public:
     OutputBuilder() : thread_([this] { loop(); }) {}
@@ -45,6 +50,7 @@ public:
             std::lock_guard<std::mutex> lock(mu_);
             stop_ = true;
         }
+        released_.store(true);
         cv_.notify_all();
         thread_.join();
     }
@@ -54,6 +60,7 @@ public:
         count_ = count;
         ready_ = false;
         requested_ = true;
+        released_.store(false);
         cv_.notify_all();
     }
 
@@ -64,35 +71,23 @@ public:
         return std::move(built_);
     }
 
+    // The call that started the build is over: the thread may stop spinning.
+    void release() { released_.store(true); }
+
 private:
+    static constexpr size_t kHugeBytes = size_t(32) << 20;
+    static constexpr std::chrono::milliseconds kActiveFor{50};
+
     static void build(std::vector<uint32_t>& v, size_t count) {
         v.reserve(count);
-        const uintptr_t huge = uintptr_t(2) << 20;
-        const uintptr_t begin = (reinterpret_cast<uintptr_t>(v.data()) + huge - 1) & ~(huge - 1);
-        const uintptr_t end = (reinterpret_cast<uintptr_t>(v.data()) + count * sizeof(uint32_t)) & ~(huge - 1);
-        if (end > begin) madvise(reinterpret_cast<void*>(begin), end - begin, MADV_HUGEPAGE);  // a hint only
+        const size_t bytes = count * sizeof(uint32_t);
+        if (bytes >= kHugeBytes) {  // a hint only; small arrays fault fast enough without it
+            const uintptr_t huge = uintptr_t(2) << 20;
+            const uintptr_t begin = (reinterpret_cast<uintptr_t>(v.data()) + huge - 1) & ~(huge - 1);
+            const uintptr_t end = (reinterpret_cast<uintptr_t>(v.data()) + bytes) & ~(huge - 1);
+            if (end > begin) madvise(reinterpret_cast<void*>(begin), end - begin, MADV_HUGEPAGE);
+        }
         v.resize(count);
-        evict_tail(v.data(), count * sizeof(uint32_t));
-    }
-
-    // The zero-fill leaves the vector's last few MB dirty in this thread's core caches. Once this
-    // thread sleeps, the copy threads' writes to those lines were slow: the last output chunk took
-    // ~300 us to copy instead of ~35 us on a B200 host. Rewriting the tail's zeros with streaming
-    // stores, which bypass and invalidate the cached copies, leaves it in memory instead.
-    static void evict_tail(uint32_t* data, size_t bytes) {
-#if defined(__x86_64__)
-        const size_t tail = std::min<size_t>(bytes, size_t(4) << 20);
-        char* from = reinterpret_cast<char*>(data) + (bytes - tail);
-        const uintptr_t aligned = (reinterpret_cast<uintptr_t>(from) + 15) & ~uintptr_t(15);
-        char* stop = reinterpret_cast<char*>(data) + bytes;
-        const __m128i zero = _mm_setzero_si128();
-        for (char* at = reinterpret_cast<char*>(aligned); at + 16 <= stop; at += 16)
-            _mm_stream_si128(reinterpret_cast<__m128i*>(at), zero);
-        _mm_sfence();
-#else
-        (void)data;
-        (void)bytes;
-#endif
     }
 
     void loop() {
@@ -109,12 +104,25 @@ private:
             built_ = std::move(v);
             ready_ = true;
             cv_.notify_all();
+            lock.unlock();
+            const auto until = std::chrono::steady_clock::now() + kActiveFor;
+            while (!released_.load(std::memory_order_acquire) && std::chrono::steady_clock::now() < until) pause();
+            lock.lock();
         }
+    }
+
+    static void pause() {
+#if defined(__x86_64__)
+        _mm_pause();
+#else
+        std::this_thread::yield();
+#endif
     }
 
     std::mutex mu_;
     std::condition_variable cv_;
     bool stop_ = false, requested_ = false, ready_ = false;
+    std::atomic<bool> released_{true};
     size_t count_ = 0;
     std::vector<uint32_t> built_;
     std::thread thread_;
@@ -161,8 +169,13 @@ fherma::Outputs fherma_run(void* opaque, const fherma::Inputs& in) {
     fherma::Outputs out;
     out.c.shape = {int64_t(state->n), int64_t(state->limbs)};
     out.c.data = state->output.take();
-    if (begun != NEGACYCLIC_OK) raise("fherma_run");
-    if (negacyclic_run_finish(state->plan, out.c.data.data()) != NEGACYCLIC_OK) raise("fherma_run");
+    if (begun != NEGACYCLIC_OK) {
+        state->output.release();
+        raise("fherma_run");
+    }
+    const int finished = negacyclic_run_finish(state->plan, out.c.data.data());
+    state->output.release();
+    if (finished != NEGACYCLIC_OK) raise("fherma_run");
     return out;
 }
 

@@ -14,10 +14,11 @@
 // job is a function of the worker index), so a job splits its work into one slice per worker.
 // A job can publish finer-grained progress itself (per-chunk counters), which is how the
 // launcher thread learns that chunk k is packed while later chunks are still being copied.
-// Waits spin for about a millisecond before they block: waking a sleeping thread goes through the
-// kernel (and, on a virtual machine's vCPUs, the hypervisor), which on the 16-vCPU host of a B200
-// box cost more than a whole small product's copies; jobs of one product come less than a
-// millisecond apart, so within a product nobody sleeps.
+// Waits spin for a fixed time (kSpinTime) before they block, and the team keeps spinning between
+// the jobs of one product: on the 16-vCPU host of a B200 box, once the copy threads slept, the
+// device's reads of host memory slowed down several-fold (the last 3.6 MB input chunk of a
+// product took 700-900 us to copy instead of 75; spinning threads keep the host's memory path
+// awake), and waking a sleeping thread goes through the kernel and the hypervisor.
 #pragma once
 
 #include <algorithm>
@@ -45,7 +46,9 @@ class HostTeam {
 public:
     using Job = std::function<void(unsigned worker, unsigned workers)>;
 
-    explicit HostTeam(unsigned workers) : workers_(std::max(1u, workers)) {
+    // spin: how long a wait spins before it blocks (see kSpinTime)
+    explicit HostTeam(unsigned workers, std::chrono::microseconds spin = kSpinTime)
+        : workers_(std::max(1u, workers)), spin_(spin) {
         for (unsigned i = 0; i < workers_; ++i) threads_.emplace_back([this, i] { loop(i); });
     }
 
@@ -78,8 +81,9 @@ public:
     // Returns once every worker has finished job `ticket` (and, jobs running in order, every
     // job posted before it).
     void wait(uint64_t ticket) {
+        const auto until = std::chrono::steady_clock::now() + spin_;
         for (uint32_t spins = 0; finished_.load(std::memory_order_acquire) < ticket; ++spins) {
-            if (spins < kSpins) {
+            if ((spins & 63u) != 63u || std::chrono::steady_clock::now() < until) {
                 NEGACYCLIC_PAUSE();
             } else {
                 std::unique_lock<std::mutex> lock(mu_);
@@ -88,7 +92,8 @@ public:
         }
     }
 
-    static constexpr uint32_t kSpins = 1u << 14;  // pause loops before blocking (~1 ms)
+    static constexpr std::chrono::microseconds kSpinTime{2000};  // default spinning before a wait blocks
+    std::chrono::microseconds spin_time() const { return spin_; }
 
     // Whether job `ticket` has finished (no waiting).
     bool finished(uint64_t ticket) const { return finished_.load(std::memory_order_acquire) >= ticket; }
@@ -122,13 +127,14 @@ private:
         uint64_t next = 1;  // ticket of the next job this worker runs
         for (;;) {
             Job job;
+            const auto until = std::chrono::steady_clock::now() + spin_;
             for (uint32_t spins = 0;; ++spins) {
                 if (posted_.load(std::memory_order_acquire) >= next) {
                     std::lock_guard<std::mutex> lock(mu_);
                     job = jobs_[next - 1 - retired_];
                     break;
                 }
-                if (spins < kSpins) {
+                if ((spins & 63u) != 63u || std::chrono::steady_clock::now() < until) {
                     NEGACYCLIC_PAUSE();
                     continue;
                 }
@@ -152,6 +158,7 @@ private:
     }
 
     const unsigned workers_;
+    const std::chrono::microseconds spin_;
     std::vector<std::thread> threads_;
     std::mutex mu_;
     std::condition_variable wake_, done_;
@@ -163,10 +170,12 @@ private:
 };
 
 // Spins until `flag` reaches `value` (acquire): one thread's short waits (the launcher waiting
-// for the team to pack a chunk); yields its core after about a millisecond.
-inline void spin_until(const std::atomic<uint32_t>& flag, uint32_t value) {
+// for the team to pack a chunk); yields its core after `spin`.
+inline void spin_until(const std::atomic<uint32_t>& flag, uint32_t value,
+                       std::chrono::microseconds spin = HostTeam::kSpinTime) {
+    const auto until = std::chrono::steady_clock::now() + spin;
     for (uint32_t spins = 0; flag.load(std::memory_order_acquire) < value; ++spins) {
-        if (spins < HostTeam::kSpins)
+        if ((spins & 63u) != 63u || std::chrono::steady_clock::now() < until)
             NEGACYCLIC_PAUSE();
         else
             std::this_thread::yield();

@@ -475,7 +475,8 @@ bool page_locked(const void* ptr) {
 }
 
 // Page-locked staging and the copy team of the host path, made on first use.
-// NEGACYCLIC_HOST_THREADS sets the team's size; by default it takes up to 6 of the host's cores.
+// NEGACYCLIC_HOST_THREADS sets the team's size (by default up to 6 of the host's cores), and
+// NEGACYCLIC_HOST_SPIN_US how long its threads spin before they sleep (default 2000 us).
 // Host memory bandwidth, shared with the copy engines and the caller's output fill, is the limit:
 // on a 16-core B200 host, fherma_run at N=65536, L=55 took 1.40-1.46 ms with 6 threads against
 // 1.52-1.62 with 8, 1.60-1.67 with 4 and 1.91 with 3 (0.65-0.77 ms at N=32768, L=28).
@@ -488,7 +489,10 @@ void ensure_staging(negacyclic_plan& s) {
         unsigned workers = std::min(6u, hw - 2);
         if (const char* env = getenv("NEGACYCLIC_HOST_THREADS"))
             workers = std::max(1u, std::min(64u, unsigned(std::strtoul(env, nullptr, 10))));
-        s.team = std::make_unique<HostTeam>(workers);
+        std::chrono::microseconds spin = HostTeam::kSpinTime;
+        if (const char* env = getenv("NEGACYCLIC_HOST_SPIN_US"))
+            spin = std::chrono::microseconds(std::min<unsigned long>(10000000ul, std::strtoul(env, nullptr, 10)));
+        s.team = std::make_unique<HostTeam>(workers, spin);
     }
 }
 
@@ -665,7 +669,7 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         for (uint32_t k = 0; k < in.size(); ++k) {
             const InChunk ch = in[k];
             const size_t host_row0 = size_t(split) * ch.j0 + ch.t, buf_row0 = size_t(ch.t) * n_sub + ch.j0;
-            spin_until(s.packed[k], pieces[k]);
+            spin_until(s.packed[k], pieces[k], s.team ? s.team->spin_time() : HostTeam::kSpinTime);
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + host_row0 * h.limbs;
                 size_t pitch = split * row;
@@ -689,7 +693,7 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
         for (uint32_t k = 0; k < in.size(); ++k) {
             const size_t first = in[k].j0, count = in[k].span, bytes = count * row;  // coefficient range
-            spin_until(s.packed[k], pieces[k]);
+            spin_until(s.packed[k], pieces[k], s.team ? s.team->spin_time() : HostTeam::kSpinTime);
             for (int op = 0; op < 2; ++op) {
                 const uint32_t* from = src[op] + first * h.limbs;
                 if (!locked[op]) from = s.stage_in + op * words + first * h.limbs;  // packed by the team

@@ -14,7 +14,9 @@
 //             callback completes the request.
 // One dispatcher thread admits queued requests in arrival order while fewer than `slots` are in
 // the pipeline and the request's operand buffers (plus any growth of the shared arena) fit the
-// HBM budget next to the resident plan tables. A request that arrives while others are on the
+// HBM budget next to the resident plan tables. With max_queue set, a submit that finds that many
+// requests already waiting is refused at once (NEGACYCLIC_EBUSY): under overload the queue, and
+// with it the latency of what is admitted, stays bounded. A request that arrives while others are on the
 // GPU joins the pipeline as soon as a place and memory free up, so its copies overlap their
 // compute. With one compute stream the CTA-pair GEMM kernel is used; concurrent launches of
 // that kernel from several streams stalled, so a process runs one server per device.
@@ -74,6 +76,8 @@ struct negacyclic_server {
     int device = 0;
     uint64_t budget = 0, resident = 0, in_flight = 0;
     uint32_t slots = 0, active = 0;  // pipeline depth, requests in it
+    uint32_t max_queue = 0;          // 0 = unbounded admission queue
+    uint64_t rejected = 0, max_queued = 0;
     std::vector<Session> sessions;
     std::deque<Request*> pending;
     std::map<uint64_t, std::unique_ptr<Request>> requests;
@@ -312,6 +316,7 @@ int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_s
     s->device = device;
     s->budget = o.hbm_budget ? o.hbm_budget : (uint64_t(60) << 30);
     s->slots = o.slots ? o.slots : 4;
+    s->max_queue = o.max_queue;
     if (s->slots > negacyclic_server::kStatusSlots) return fail(NEGACYCLIC_EINVAL, "at most 1024 slots");
     DeviceGuard guard(device);
     try {
@@ -370,6 +375,10 @@ int negacyclic_server_submit(negacyclic_server* s, uint32_t session, uint32_t n,
     if (!s || !a || !b || !c || !request) return fail(NEGACYCLIC_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lock(s->mu);
     if (session >= s->sessions.size()) return fail(NEGACYCLIC_EINVAL, "unknown session");
+    if (s->max_queue && s->pending.size() >= s->max_queue) {
+        ++s->rejected;
+        return fail(NEGACYCLIC_EBUSY, "request queue full");
+    }
     auto r = std::make_unique<Request>();
     r->id = s->next_id++;
     r->session = session;
@@ -382,6 +391,7 @@ int negacyclic_server_submit(negacyclic_server* s, uint32_t session, uint32_t n,
     if (s->first_submit == 0) s->first_submit = r->submitted;
     *request = r->id;
     s->pending.push_back(r.get());
+    s->max_queued = std::max<uint64_t>(s->max_queued, s->pending.size());
     s->requests.emplace(r->id, std::move(r));
     s->wake.notify_one();
     return NEGACYCLIC_OK;
@@ -415,6 +425,8 @@ int negacyclic_server_get_stats(negacyclic_server* s, negacyclic_server_stats* o
     out->queued = s->pending.size();
     out->resident_bytes = s->resident + s->arena_bytes;
     out->in_flight_bytes = s->in_flight;
+    out->rejected = s->rejected;
+    out->max_queued = s->max_queued;
     std::vector<double> lat = s->latencies;
     if (!lat.empty()) {
         std::sort(lat.begin(), lat.end());

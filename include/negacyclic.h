@@ -40,6 +40,7 @@ extern "C" {
 #define NEGACYCLIC_ECUDA 4      /* a CUDA runtime/driver call failed (src/solve.cu:32-34) */
 #define NEGACYCLIC_ENOMEM 5     /* device or pinned host allocation failed */
 #define NEGACYCLIC_ENODEV 6     /* no usable sm_100 device */
+#define NEGACYCLIC_EBUSY 7      /* serving form: the request queue is full; the request was not taken */
 
 /* Bits of a plan's device status word (negacyclic_plan_status, negacyclic_batch_status). The
  * reference has no device-side error word: its waits are unbounded and its reduction has no
@@ -261,9 +262,12 @@ int negacyclic_gemm_u8(const uint8_t* d_a, const uint8_t* d_b, int32_t* d_d, uin
  * Batched form: many products of uneven (N, W, q) in one graph launch.
  * New in this library (the reference runs one product per harness call,
  * src/main.cpp:164-204). Instances are planned individually (an autotuner picks
- * each shape's ring split and GEMM kernel by timing them, cached in a text file),
- * assigned longest-first to compute lanes (one by default) that share one work
- * arena each, and captured into a single CUDA graph.
+ * each shape's ring split and GEMM kernel by timing them, cached in a text file)
+ * and captured into a single CUDA graph. By default the graph has two phases:
+ * instances under about 1 ms of device time share the GPU on up to four compute
+ * lanes (single-CTA tensor GEMMs), then the larger ones run one after another on
+ * lane 0 with CTA-pair GEMMs. lanes > 0 instead spreads every instance over that
+ * many lanes. Each lane shares one work arena among its instances.
  */
 typedef struct negacyclic_batch negacyclic_batch;
 
@@ -273,7 +277,8 @@ typedef struct {
 } negacyclic_point;
 
 typedef struct {
-    uint32_t lanes;          /* concurrent compute streams; 0 = 1 (lanes > 1 use single-CTA GEMM tiles) */
+    uint32_t lanes;          /* 0 = two phases (see above); else every instance on this many streams
+                                (single-CTA GEMM tiles when more than one) */
     uint32_t tune;           /* 1: time candidate configurations for shapes not in the cache */
     int32_t device;          /* -1 = current device */
     uint32_t reserved0;
@@ -286,6 +291,8 @@ typedef struct {
     uint32_t lane;           /* stream it runs on */
     uint32_t requested_gemm; /* NEGACYCLIC_GEMM_* chosen by the tuner (0 = default) */
     double tuned_ms;         /* measured device time of one product (0 = not tuned) */
+    uint32_t phase;          /* 0: runs concurrently with others; 1: runs alone, after phase 0 */
+    uint32_t reserved;
 } negacyclic_batch_instance;
 
 int negacyclic_batch_create(const negacyclic_point* points, uint32_t count,
@@ -338,7 +345,9 @@ typedef struct {
     uint64_t hbm_budget;  /* bytes for resident plan tables + in-flight requests; 0 = 60 GiB */
     uint32_t slots;       /* concurrent requests (streams); 0 = 4 */
     int32_t device;       /* -1 = current device */
-    uint32_t reserved[4];
+    uint32_t max_queue;   /* requests waiting for admission beyond which submit refuses new ones
+                             (NEGACYCLIC_EBUSY); 0 = no limit */
+    uint32_t reserved[3];
 } negacyclic_server_options;
 
 typedef struct {
@@ -346,6 +355,8 @@ typedef struct {
     uint64_t resident_bytes, in_flight_bytes;
     double p50_ms, p99_ms, mean_ms;  /* submit -> result on the host, completed requests */
     double products_per_s;           /* completed / (last finish - first submit) */
+    uint64_t rejected;               /* submits refused because the queue was full */
+    uint64_t max_queued;             /* deepest the admission queue has been */
 } negacyclic_server_stats;
 
 int negacyclic_server_create(const negacyclic_server_options* opts, negacyclic_server** server);
@@ -359,6 +370,8 @@ int negacyclic_server_open_session(negacyclic_server* server, uint32_t w, uint32
                                    const uint32_t* q, const uint32_t* ns, uint32_t count,
                                    uint32_t* session);
 
+/* Queues a request and returns at once; NEGACYCLIC_EBUSY (nothing queued) when max_queue requests
+ * already wait for admission. */
 int negacyclic_server_submit(negacyclic_server* server, uint32_t session, uint32_t n,
                              const uint32_t* a, const uint32_t* b, uint32_t* c, uint64_t* request);
 

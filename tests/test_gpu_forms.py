@@ -58,15 +58,41 @@ def test_batch_graph_matches_oracle_and_plain_path(fpc, inputs, oracle, cudart):
         assert lanes == {0, 1, 2}
 
 
-def test_batch_default_single_lane_pipeline(fpc, inputs, oracle):
+def test_batch_single_lane_pipeline(fpc, inputs, oracle):
     """One compute lane (CTA-pair GEMMs) with copy-in / copy-out streams, host arrays in and out."""
     points = uneven_points(inputs, 8, 13, sizes=(1024, 4096, 8192), limb_range=(16, 300))
-    with fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in points]) as batch:
+    with fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in points], lanes=1) as batch:
         assert {batch.info(i)["lane"] for i in range(len(points))} == {0}
         for _ in range(2):
             results = batch.run([p[3] for p in points], [p[4] for p in points])
             for (n, l, q, a, b), c in zip(points, results):
                 assert np.array_equal(c, oracle.kronecker(q, a, b)), (n, l)
+
+
+def test_batch_two_phases_by_default(fpc, inputs, oracle, cudart):
+    """Default lanes: small instances share the GPU on several lanes (single-CTA GEMMs), then the
+    large one runs alone on lane 0 with CTA-pair GEMMs; device graph and host arrays both exact."""
+    points = uneven_points(inputs, 9, 17, sizes=(1024, 2048, 4096), limb_range=(8, 90))
+    q, a, b = inputs.instance(65536, 300, 1717, 0)  # estimated at well over 1 ms: the sequential phase
+    points.append((65536, 300, q, a, b))
+    with fpc.Batch([(n, 32 * l, l, q) for n, l, q, _, _ in points]) as batch:
+        lanes = [batch.info(i)["lane"] for i in range(len(points))]
+        assert len(set(lanes[:-1])) > 1 and lanes[-1] == 0, lanes
+        assert batch.info(len(points) - 1)["gemm"] == 3
+        want = [oracle.kronecker(q, a, b) for _, _, q, a, b in points]
+        for i, (n, l, q, a, b) in enumerate(points):
+            da, db, _ = batch.io(i)
+            assert cudart.cudaMemcpy(da, a.ctypes.data, a.nbytes, H2D) == 0
+            assert cudart.cudaMemcpy(db, b.ctypes.data, b.nbytes, H2D) == 0
+        batch.run_device(0)
+        assert not batch.status().any()
+        for i, (n, l, q, a, b) in enumerate(points):
+            c = np.empty_like(a)
+            assert cudart.cudaMemcpy(c.ctypes.data, batch.io(i)[2], c.nbytes, D2H) == 0
+            assert np.array_equal(c, want[i]), (i, n, l)
+        results = batch.run([p[3] for p in points], [p[4] for p in points])
+        for i, c in enumerate(results):
+            assert np.array_equal(c, want[i]), i
 
 
 def test_batch_host_path_and_autotuner(fpc, inputs, oracle, tmp_path):
@@ -124,3 +150,27 @@ def test_server_admission_respects_the_budget(fpc, inputs):
         with pytest.raises(RuntimeError, match="budget"):
             server.wait(server.submit(session, big, big))
         assert server.stats()["failed"] == 1
+
+
+def test_server_refuses_beyond_its_queue_bound(fpc, inputs):
+    """Under overload the serving form sheds load at submit (NEGACYCLIC_EBUSY) instead of letting
+    its queue grow: with one slot and a queue bound of two, a burst is partly refused, the rest
+    completes, and the stats count both and the deepest queue seen."""
+    limbs = 64
+    q = inputs.random_modulus(limbs, 202)
+    rng = np.random.Generator(np.random.PCG64(9))
+    a = inputs.random_operand(rng, 65536, q)
+    b = inputs.random_operand(rng, 65536, q)
+    with fpc.Server(slots=1, max_queue=2, hbm_budget=8 << 30) as server:
+        session = server.open_session(32 * limbs, limbs, q, ns=[65536])
+        first, _ = server.wait(server.submit(session, a, b))  # warm
+        ids = [server.submit(session, a, b) for _ in range(24)]
+        accepted = [rid for rid in ids if rid is not None]
+        assert 0 < len(accepted) < len(ids)
+        for rid in accepted:
+            c, _ = server.wait(rid)
+            assert np.array_equal(c, first)
+        stats = server.stats()
+    assert stats["rejected"] == len(ids) - len(accepted)
+    assert stats["completed"] == 1 + len(accepted) and stats["failed"] == 0
+    assert 1 <= stats["max_queued"] <= 2
