@@ -127,6 +127,19 @@ def test_random_points_against_oracle(n, limbs, split, fpc, inputs, oracle):
             assert np.array_equal(got, want), (n, limbs, split, engine, index)
 
 
+@pytest.mark.parametrize("limbs", [3, 40])
+def test_every_ring_split(limbs, fpc, inputs, oracle):
+    """Ring splits 1 to 16 at N=8192 (transforms of 8192 down to 512 points, pointwise combines
+    of 1 to 16 transforms): each gives the oracle's product."""
+    n = 8192
+    q, a, b = inputs.instance(n, limbs, 4242, 0)
+    want = oracle.kronecker(q, a, b)
+    for split in (1, 2, 4, 8, 16):
+        with fpc.Plan(n, 32 * limbs, limbs, q, split=split) as plan:
+            assert plan.info()["split"] == split
+            assert np.array_equal(plan.run(a, b), want), split
+
+
 def test_small_moduli(fpc, inputs, oracle):
     """q of one or two limbs, including q below a prime and q = 2, 3."""
     rng = np.random.Generator(np.random.PCG64(3))
