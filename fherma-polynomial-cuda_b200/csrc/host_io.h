@@ -18,7 +18,10 @@
 // the jobs of one product: on the 16-vCPU host of a B200 box, once the copy threads slept, the
 // device's reads of host memory slowed down several-fold (the last 3.6 MB input chunk of a
 // product took 700-900 us to copy instead of 75; spinning threads keep the host's memory path
-// awake), and waking a sleeping thread goes through the kernel and the hypervisor.
+// awake), and waking a sleeping thread goes through the kernel and the hypervisor. The default
+// spin (100 ms) also spans the platform harness's file I/O between two calls: behind that
+// harness, fherma_run took 0.523 ms against 0.535 at N=32768/L=28, and 1.49 against 1.54 at
+// N=65536/L=55, with 100 ms instead of 2 ms (4 alternating runs of 20 cases each).
 #pragma once
 
 #include <algorithm>
@@ -56,6 +59,7 @@ public:
         {
             std::lock_guard<std::mutex> lock(mu_);
             stop_ = true;
+            stopping_.store(true, std::memory_order_release);  // ends spinning waits at once
         }
         wake_.notify_all();
         for (auto& t : threads_) t.join();
@@ -92,7 +96,7 @@ public:
         }
     }
 
-    static constexpr std::chrono::microseconds kSpinTime{2000};  // default spinning before a wait blocks
+    static constexpr std::chrono::microseconds kSpinTime{100000};  // default spinning before a wait blocks
     std::chrono::microseconds spin_time() const { return spin_; }
 
     // Whether job `ticket` has finished (no waiting).
@@ -134,6 +138,9 @@ private:
                     job = jobs_[next - 1 - retired_];
                     break;
                 }
+                // stopping and nothing left (the acquire makes every earlier post visible)
+                if (stopping_.load(std::memory_order_acquire) && posted_.load(std::memory_order_acquire) < next)
+                    return;
                 if ((spins & 63u) != 63u || std::chrono::steady_clock::now() < until) {
                     NEGACYCLIC_PAUSE();
                     continue;
@@ -167,6 +174,7 @@ private:
     std::atomic<uint64_t> posted_{0}, finished_{0};
     std::map<uint64_t, unsigned> count_;  // workers done, per job still running
     bool stop_ = false;
+    std::atomic<bool> stopping_{false};
 };
 
 // Spins until `flag` reaches `value` (acquire): one thread's short waits (the launcher waiting

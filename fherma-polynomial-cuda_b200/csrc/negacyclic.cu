@@ -476,7 +476,7 @@ bool page_locked(const void* ptr) {
 
 // Page-locked staging and the copy team of the host path, made on first use.
 // NEGACYCLIC_HOST_THREADS sets the team's size (by default up to 6 of the host's cores), and
-// NEGACYCLIC_HOST_SPIN_US how long its threads spin before they sleep (default 2000 us).
+// NEGACYCLIC_HOST_SPIN_US how long its threads spin before they sleep (default 100000 us).
 // Host memory bandwidth, shared with the copy engines and the caller's output fill, is the limit:
 // on a 16-core B200 host, fherma_run at N=65536, L=55 took 1.40-1.46 ms with 6 threads against
 // 1.52-1.62 with 8, 1.60-1.67 with 4 and 1.91 with 3 (0.65-0.77 ms at N=32768, L=28).
@@ -610,6 +610,8 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         s.team->wait(s.pack_ticket);
         s.pack_ticket = 0;
     }
+    if (!s.status_host) check(cudaHostAlloc(&s.status_host, 64, cudaHostAllocDefault), "cudaHostAlloc");
+    *static_cast<volatile uint32_t*>(s.status_host) = 0;  // the previous call's stream has finished
     check(cudaMemsetAsync(s.status, 0, 4, st), "memset");
     const uint32_t* src[2] = {a, b};
     const bool locked[2] = {a_locked, b_locked};
@@ -736,6 +738,8 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
             check(cudaEventRecord(s.copied_out[k - 1], s.copy_out), "cudaEventRecord");
         }
     }
+    // every kernel that writes the status word runs on st: its copy follows the last of them
+    check(cudaMemcpyAsync(s.status_host, s.status, 4, cudaMemcpyDeviceToHost, st), "status word");
     check(cudaGetLastError(), "product kernels");
 }
 
@@ -775,8 +779,7 @@ int host_finish(negacyclic_plan& s, uint32_t* c) {
     }
     check(cudaStreamSynchronize(s.copy_out), "product");
     check(cudaStreamSynchronize(s.stream), "product");
-    uint32_t flags = 0;  // every kernel that writes the status word ran on s.stream
-    check(cudaMemcpy(&flags, s.status, 4, cudaMemcpyDeviceToHost), "status word");
+    const uint32_t flags = *static_cast<volatile const uint32_t*>(s.status_host);  // landed with s.stream
     return status_failure(flags);
 }
 

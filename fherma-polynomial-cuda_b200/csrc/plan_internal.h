@@ -44,6 +44,9 @@ struct negacyclic_plan {
     // host path with pageable arrays: page-locked staging and a copy team (made on first use)
     uint32_t* stage_in = nullptr;   // [2][N][L], write-combined
     uint32_t* stage_out = nullptr;  // [N][L]
+    // the host path's copy of the status word, written on `stream` after the last kernel, so
+    // that reading it costs no extra round trip once the stream has finished
+    uint32_t* status_host = nullptr;
     std::unique_ptr<negacyclic::HostTeam> team;
     std::atomic<uint32_t> packed[kMaxChunks] = {};  // pieces of input chunk k packed
     std::atomic<uint32_t> next_piece{0};            // next unclaimed piece of the running pack job
@@ -70,6 +73,7 @@ struct negacyclic_plan {
         }
         if (stage_in) cudaFreeHost(stage_in);
         if (stage_out) cudaFreeHost(stage_out);
+        if (status_host) cudaFreeHost(status_host);
         team.reset();
         if (stream) cudaStreamDestroy(stream);
         if (copy_in) cudaStreamDestroy(copy_in);
