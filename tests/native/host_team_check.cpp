@@ -1,12 +1,14 @@
 // CPU check of the host path's copy team (fherma-polynomial-cuda_b200/csrc/host_io.h), built and
 // run by tests/test_host_team.py: a pack job that publishes per-chunk counters while a launcher
 // thread consumes chunks in order, an unpack job that follows per-chunk "landed" flags, blocking
-// copies and touches, and many calls in a row with idle gaps (workers going to sleep and waking).
+// copies and touches, and many calls in a row with idle gaps (with a short spin, workers going to
+// sleep and waking), then that a team whose workers are spinning is destroyed at once.
 #include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <random>
 #include <thread>
 #include <vector>
@@ -24,10 +26,8 @@ static int failures = 0;
         }                                                                     \
     } while (0)
 
-int main(int argc, char** argv) {
-    const unsigned workers = argc > 1 ? unsigned(std::atoi(argv[1])) : 5;
-    HostTeam team(workers);
-    std::mt19937_64 rng(7);
+static void run_calls(HostTeam& team, uint64_t seed) {
+    std::mt19937_64 rng(seed);
     constexpr uint32_t kChunks = 16;
     for (int call = 0; call < 300; ++call) {
         const uint32_t limbs = 1 + uint32_t(rng() % 70), split = 1u << (rng() % 4);
@@ -82,7 +82,30 @@ int main(int argc, char** argv) {
         EXPECT(copy == src);
         team.touch(copy.data(), copy.size() * 4);
         EXPECT(std::all_of(copy.begin(), copy.end(), [](uint32_t x) { return x == 0; }));
-        if (call % 50 == 49) std::this_thread::sleep_for(std::chrono::milliseconds(20));  // workers fall asleep
+        if (call % 50 == 49) std::this_thread::sleep_for(std::chrono::milliseconds(20));  // past a short spin
+    }
+}
+
+int main(int argc, char** argv) {
+    const unsigned workers = argc > 1 ? unsigned(std::atoi(argv[1])) : 5;
+    {
+        HostTeam team(workers);  // default spin: the workers stay awake between calls
+        run_calls(team, 7);
+    }
+    {
+        HostTeam team(workers, std::chrono::microseconds(200));  // workers sleep in the idle gaps
+        run_calls(team, 8);
+    }
+    {  // destroying a team whose workers are spinning does not wait out their spin
+        auto team = std::make_unique<HostTeam>(workers);
+        std::vector<uint32_t> a(1 << 16, 1u), b(a.size(), 0u);
+        team->copy(b.data(), a.data(), a.size() * 4);
+        EXPECT(a == b);
+        const auto start = std::chrono::steady_clock::now();
+        team.reset();
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
+        const double spin_ms = std::chrono::duration<double, std::milli>(HostTeam::kSpinTime).count();
+        EXPECT(ms < 0.5 * spin_ms);
     }
     std::printf("host team check: %d failures\n", failures);
     return failures ? 1 : 0;
