@@ -890,7 +890,8 @@ bool gemm_tensor_accepts(const TensorGemmPlan& plan, const RowMap& rows, uint32_
     if (!plan.ready || rows.mode != plan.rows.mode) return false;
     if (rows.mode == kRowsSplit)
         return rows.span % kBlockM == 0 && rows.first % kBlockM == 0 && rows.first + rows.span <= plan.rows.n_sub &&
-               rows.t_first + rows.t_count <= plan.rows.split && m == 2 * rows.t_count * rows.span;
+               rows.t_first + rows.t_count <= plan.rows.split && m % (rows.t_count * rows.span) == 0 &&
+               rows.op_first + m / (rows.t_count * rows.span) <= 2;
     return uint64_t(rows.first) + m <= plan.m;
 }
 

@@ -49,17 +49,17 @@ __global__ void pad_operands_kernel(const uint32_t* __restrict__ a, const uint32
     }
 }
 
-// Rows [first, first + count) of both operands (operand stride N rows) from an unpadded [2][N][L]
-// array into the padded split-major layout. Staged rows are either already split-major
-// (log_split = 0: row = position) or in coefficient order (row i goes to t*N' + j, i = s*j + t).
-// One warp per row.
+// Rows [first, first + count) of operands [op_first, op_first + op_count) (operand stride N rows)
+// from an unpadded [2][N][L] array into the padded split-major layout. Staged rows are either
+// already split-major (log_split = 0: row = position) or in coefficient order (row i goes to
+// t*N' + j, i = s*j + t). One warp per row.
 __global__ void pad_rows_kernel(const uint32_t* __restrict__ staged, uint32_t* __restrict__ out, uint32_t n,
                                 uint32_t limbs, uint32_t padded, uint32_t log_split, uint32_t log_n_sub,
-                                uint32_t first, uint32_t count) {
+                                uint32_t first, uint32_t count, uint32_t op_first, uint32_t op_count) {
     const uint32_t lane = threadIdx.x % 32, warps = gridDim.x * (blockDim.x / 32);
     const uint32_t split_mask = (1u << log_split) - 1;
-    for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < 2 * count; w += warps) {
-        const uint32_t op = w >= count ? 1 : 0, i = first + (w - op * count);
+    for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < op_count * count; w += warps) {
+        const uint32_t local_op = w / count, op = op_first + local_op, i = first + (w - local_op * count);
         const uint32_t row = ((i & split_mask) << log_n_sub) + (i >> log_split);
         pad_row(staged + (size_t(op) * n + i) * limbs, out + (size_t(op) * n + row) * padded, limbs, padded, lane);
     }
@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const uint8_t* __restric
 
 __global__ void __launch_bounds__(512) ntt_forward_kernel(uint32_t* residues, const DevicePrime* __restrict__ primes,
                                                           const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
-                                                          uint32_t n_sub, uint32_t t_first) {
+                                                          uint32_t n_sub, uint32_t t_first, uint32_t op_first) {
     extern __shared__ uint32_t x[];
-    const uint32_t t_index = t_first + blockIdx.x, k = blockIdx.y, op = blockIdx.z;
+    const uint32_t t_index = t_first + blockIdx.x, k = blockIdx.y, op = op_first + blockIdx.z;
     const uint32_t p = primes[k].p;
     uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * n_sub;
     const uint2* table = fwd + size_t(k) * n_sub;
@@ -418,15 +418,16 @@ __device__ __forceinline__ void ntt_passes(uint32_t* data, uint32_t* xs, const u
     }
 }
 
-// grid (2 t_count, r): x = op*t_count + (t - t_first), y = prime, so a prime's transforms
-// share its twiddles in L2
+// grid (op_count t_count, r): x = (op - op_first)*t_count + (t - t_first), y = prime, so a prime's
+// transforms share its twiddles in L2
 template <uint32_t kLog>
 __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_forward_blocked_kernel(
     uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ fwd, uint32_t r, uint32_t n,
-    uint32_t t_first, uint32_t t_count) {
+    uint32_t t_first, uint32_t t_count, uint32_t op_first) {
     extern __shared__ uint32_t xs[];
     constexpr uint32_t kN = 1u << kLog;
-    const uint32_t op = blockIdx.x / t_count, t_index = t_first + blockIdx.x - op * t_count, k = blockIdx.y;
+    const uint32_t local_op = blockIdx.x / t_count, op = op_first + local_op;
+    const uint32_t t_index = t_first + blockIdx.x - local_op * t_count, k = blockIdx.y;
     uint32_t* data = residues + (size_t(op) * r + k) * n + size_t(t_index) * kN;
     ntt_passes<true, kLog, 0>(data, xs, fwd + size_t(k) * kN, primes[k].p, 0, 0);
 }
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_fo
 template <uint32_t kLog>
 __global__ void __launch_bounds__(1u << (kLog - 4), (kLog >= 13 ? 2 : 4)) ntt_inverse_blocked_kernel(
     uint32_t* residues, const DevicePrime* __restrict__ primes, const uint2* __restrict__ inv, uint32_t r, uint32_t n,
-    uint32_t v_first, uint32_t v_count) {
+    uint32_t v_first, uint32_t v_count, uint32_t /*op_first: the inverse works on operand row 0 only*/) {
     extern __shared__ uint32_t xs[];
     constexpr uint32_t kN = 1u << kLog;
     const uint32_t v_index = v_first + blockIdx.x, k = blockIdx.y;
@@ -760,11 +761,12 @@ void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, ui
 }
 
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream) {
+                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream, uint32_t op_first,
+                     uint32_t op_count) {
     const uint32_t log_split = log2_u32(split), log_n_sub = log2_u32(n) - log_split;
-    const uint32_t blocks = std::min<uint32_t>((2 * count + 7) / 8, 148 * 16);
+    const uint32_t blocks = std::min<uint32_t>((op_count * count + 7) / 8, 148 * 16);
     pad_rows_kernel<<<blocks, 256, 0, stream>>>(staged, out, n, limbs, padded_limbs, log_split, log_n_sub, first_row,
-                                                count);
+                                                count, op_first, op_count);
 }
 
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv, uint2* zeta,
@@ -798,7 +800,7 @@ static uint32_t ntt_threads(uint32_t n_sub) {
 
 template <bool kForward, uint32_t kLog>
 static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const uint2* table, uint32_t r, uint32_t n,
-                           uint32_t first, uint32_t count, cudaStream_t stream) {
+                           uint32_t first, uint32_t count, cudaStream_t stream, uint32_t op_first, uint32_t op_count) {
     constexpr uint32_t kN = 1u << kLog;
     const size_t smem = kN * sizeof(uint32_t);
     auto kernel = kForward ? ntt_forward_blocked_kernel<kLog> : ntt_inverse_blocked_kernel<kLog>;
@@ -807,30 +809,36 @@ static void launch_blocked(uint32_t* residues, const DevicePrime* primes, const 
         cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         configured = true;
     }
-    dim3 grid(kForward ? 2 * count : count, r);
-    kernel<<<grid, kN / kPerThread, smem, stream>>>(residues, primes, table, r, n, first, count);
+    dim3 grid(kForward ? op_count * count : count, r);
+    kernel<<<grid, kN / kPerThread, smem, stream>>>(residues, primes, table, r, n, first, count, op_first);
 }
 
 template <bool kForward>
 static bool launch_blocked_any(uint32_t n_sub, uint32_t* residues, const DevicePrime* primes, const uint2* table,
-                               uint32_t r, uint32_t n, uint32_t first, uint32_t count, cudaStream_t stream) {
+                               uint32_t r, uint32_t n, uint32_t first, uint32_t count, cudaStream_t stream,
+                               uint32_t op_first = 0, uint32_t op_count = 2) {
+#define NEGACYCLIC_BLOCKED(LOG) \
+    launch_blocked<kForward, LOG>(residues, primes, table, r, n, first, count, stream, op_first, op_count)
     switch (n_sub) {
-        case 256: launch_blocked<kForward, 8>(residues, primes, table, r, n, first, count, stream); return true;
-        case 512: launch_blocked<kForward, 9>(residues, primes, table, r, n, first, count, stream); return true;
-        case 1024: launch_blocked<kForward, 10>(residues, primes, table, r, n, first, count, stream); return true;
-        case 2048: launch_blocked<kForward, 11>(residues, primes, table, r, n, first, count, stream); return true;
-        case 4096: launch_blocked<kForward, 12>(residues, primes, table, r, n, first, count, stream); return true;
-        case 8192: launch_blocked<kForward, 13>(residues, primes, table, r, n, first, count, stream); return true;
+        case 256: NEGACYCLIC_BLOCKED(8); return true;
+        case 512: NEGACYCLIC_BLOCKED(9); return true;
+        case 1024: NEGACYCLIC_BLOCKED(10); return true;
+        case 2048: NEGACYCLIC_BLOCKED(11); return true;
+        case 4096: NEGACYCLIC_BLOCKED(12); return true;
+        case 8192: NEGACYCLIC_BLOCKED(13); return true;
         default: return false;
     }
+#undef NEGACYCLIC_BLOCKED
 }
 
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r, uint32_t n,
-                        uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream) {
-    if (launch_blocked_any<true>(n_sub, residues, primes, fwd, r, n, t_first, t_count, stream)) return;
-    dim3 grid(t_count, r, 2);
+                        uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream, uint32_t op_first,
+                        uint32_t op_count) {
+    if (launch_blocked_any<true>(n_sub, residues, primes, fwd, r, n, t_first, t_count, stream, op_first, op_count))
+        return;
+    dim3 grid(t_count, r, op_count);
     ntt_forward_kernel<<<grid, ntt_threads(n_sub), n_sub * sizeof(uint32_t), stream>>>(residues, primes, fwd, r, n,
-                                                                                          n_sub, t_first);
+                                                                                          n_sub, t_first, op_first);
 }
 
 void launch_ntt_inverse(uint32_t* residues, const DevicePrime* primes, const uint2* inv, uint32_t r, uint32_t n,

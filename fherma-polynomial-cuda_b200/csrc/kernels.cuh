@@ -9,7 +9,7 @@ namespace negacyclic {
 
 // Row addressing of the u8 GEMM's A operand, for one launch (a whole product or a chunk).
 //  kRowsLinear: GEMM row m reads operand row first + m.
-//  kRowsSplit:  GEMM row m = op*(t_count*span) + (t - t_first)*span + (j - first),
+//  kRowsSplit:  GEMM row m = (op - op_first)*(t_count*span) + (t - t_first)*span + (j - first),
 //               t in [t_first, t_first + t_count), j in [first, first + span), covers
 //               coefficient i = s*j + t of operand op, which the pad kernels store
 //               split-major at operand row op*N + t*N' + j, and produces residue row op,
@@ -24,16 +24,17 @@ struct RowMap {
     uint32_t span;     // split: j values per (operand, t) in this launch
     uint32_t t_first;  // split: transforms [t_first, t_first + t_count) in this launch
     uint32_t t_count;
+    uint32_t op_first = 0;  // split: first operand (0: a, 1: b); m / (t_count*span) operands
 
     static RowMap linear(uint32_t first_row) { return RowMap{kRowsLinear, 0, 0, 1, first_row, 0, 0, 1}; }
     static RowMap split_rows(uint32_t n, uint32_t n_sub, uint32_t split, uint32_t first_j, uint32_t j_span,
-                             uint32_t t_first, uint32_t t_count) {
-        return RowMap{kRowsSplit, n, n_sub, split, first_j, j_span, t_first, t_count};
+                             uint32_t t_first, uint32_t t_count, uint32_t op_first = 0) {
+        return RowMap{kRowsSplit, n, n_sub, split, first_j, j_span, t_first, t_count, op_first};
     }
     __host__ __device__ __forceinline__ void decompose(uint32_t m, uint32_t& op, uint32_t& t, uint32_t& j) const {
-        const uint32_t per_op = t_count * span;
-        op = m / per_op;
-        const uint32_t rem = m - op * per_op;
+        const uint32_t per_op = t_count * span, local_op = m / per_op;
+        op = op_first + local_op;
+        const uint32_t rem = m - local_op * per_op;
         const uint32_t dt = rem / span;
         t = t_first + dt;
         j = first + (rem - dt * span);
@@ -79,11 +80,12 @@ struct Epilogue {
 // limbs padded with zeros to Lp
 void launch_pad_operands(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n,
                          uint32_t limbs, uint32_t padded_limbs, uint32_t split, cudaStream_t stream);
-// rows [first_row, first_row + count) of both operands (operand stride N rows) from an unpadded
-// [2][N][L] array into the padded split-major [2][N][Lp] layout: staged in coefficient order
-// (split = s, rows are permuted) or already split-major (split = 1)
+// rows [first_row, first_row + count) of operands [op_first, op_first + op_count) (operand stride N
+// rows) from an unpadded [2][N][L] array into the padded split-major [2][N][Lp] layout: staged in
+// coefficient order (split = s, rows are permuted) or already split-major (split = 1)
 void launch_pad_rows(const uint32_t* staged, uint32_t* out, uint32_t n, uint32_t limbs, uint32_t padded_limbs,
-                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream);
+                     uint32_t split, uint32_t first_row, uint32_t count, cudaStream_t stream, uint32_t op_first = 0,
+                     uint32_t op_count = 2);
 void launch_twiddles(const DevicePrime* primes, uint32_t r, uint32_t n_sub, uint2* fwd, uint2* inv,
                      uint2* zeta, cudaStream_t stream);
 void launch_convert_weights(const DevicePrime* primes, uint32_t r, uint32_t padded_r, uint32_t limbs,
@@ -92,9 +94,11 @@ void launch_crt_weights(const uint32_t* weights_words, uint32_t r, uint32_t padd
                         uint32_t columns, uint8_t* out, cudaStream_t stream);
 void launch_gemm_simt(const uint8_t* a, uint64_t a_pitch, RowMap rows, uint32_t m, const uint8_t* b,
                       uint32_t columns, uint32_t k_bytes, const Epilogue& epilogue, cudaStream_t stream);
-// forward NTTs of transforms [t_first, t_first + t_count) of both operands, every prime
+// forward NTTs of transforms [t_first, t_first + t_count) of operands [op_first, op_first + op_count),
+// every prime
 void launch_ntt_forward(uint32_t* residues, const DevicePrime* primes, const uint2* fwd, uint32_t r,
-                        uint32_t n, uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream);
+                        uint32_t n, uint32_t n_sub, uint32_t t_first, uint32_t t_count, cudaStream_t stream,
+                        uint32_t op_first = 0, uint32_t op_count = 2);
 void launch_pointwise(uint32_t* residues, const DevicePrime* primes, const uint2* zeta, uint32_t r,
                       uint32_t n, uint32_t n_sub, uint32_t split, cudaStream_t stream);
 // inverse NTTs of transforms [v_first, v_first + v_count), every prime

@@ -59,9 +59,9 @@ namespace negacyclic::detail {
 constexpr uint32_t kStages = 7;  // convert, forward, pointwise, inverse, transpose, crt, reduce
 
 // conversion GEMM over the coefficients s*j + t, t in [t_first, t_first + t_count),
-// j in [first_j, first_j + span), both operands
+// j in [first_j, first_j + span), of operands [op_first, op_first + op_count)
 void enqueue_convert(negacyclic_plan& s, uint32_t t_first, uint32_t t_count, uint32_t first_j, uint32_t span,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, uint32_t op_first = 0, uint32_t op_count = 2) {
     const HostPlan& h = s.host;
     Epilogue convert{};
     convert.mode = kEpilogueConvert;
@@ -70,8 +70,8 @@ void enqueue_convert(negacyclic_plan& s, uint32_t t_first, uint32_t t_count, uin
     convert.r = s.r;
     convert.n = h.n;
     convert.status = s.status;
-    const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span, t_first, t_count);
-    const uint32_t m = 2 * t_count * span;
+    const RowMap rows = RowMap::split_rows(h.n, h.n_sub, h.split, first_j, span, t_first, t_count, op_first);
+    const uint32_t m = op_count * t_count * span;
     if (s.convert_engine == NEGACYCLIC_GEMM_TENSOR && gemm_tensor_accepts(s.convert_gemm, rows, m))
         launch_gemm_tensor(s.convert_gemm, convert, stream, rows, m);
     else
@@ -505,6 +505,8 @@ void ensure_staging(negacyclic_plan& s) {
 // and reduction.
 struct InChunk {  // transform t, positions j in [j0, j0 + span): coefficients s*j + t
     uint32_t t, j0, span;
+    uint32_t op = kBothOperands;  // operand 0 (a) or 1 (b), or both
+    static constexpr uint32_t kBothOperands = 2;
 };
 struct OutChunk {  // coefficients [first, first + count)
     uint32_t first, count;
@@ -556,12 +558,16 @@ void stream_chunks(const negacyclic_plan& s, bool ordered, std::vector<InChunk>&
         else
             in.push_back(InChunk{0, (s.chunks - 1) * per, per});
     } else {
-        // narrow rows: about 2 MB of input per chunk (at least two chunks, at most s.chunks, and at
-        // least 256 positions of every transform each). Small copies carry fixed costs: 0.46 MB
-        // host-to-device copies ran at 23 GB/s against 55 for large ones (N=32768, L=28).
-        const uint32_t count = chunk_count(size_t(2) * h.n * h.limbs * 4, 2u << 20, s.chunks, n_sub / 256);
+        // narrow rows: operand a, then operand b, each in coefficient ranges of about 1 MB (at
+        // least two per operand, and at least 256 positions of every transform each), so that a's
+        // conversion and forward NTTs run while b is still on the way. Small copies carry fixed
+        // costs: 0.46 MB host-to-device copies ran at 23 GB/s against 55 for large ones (N=32768,
+        // L=28).
+        const uint32_t count = chunk_count(size_t(h.n) * h.limbs * 4, 1u << 20, std::min(s.chunks, kMax / 2),
+                                           n_sub / 256);
         const uint32_t span = h.n / count;
-        for (uint32_t k = 0; k < count; ++k) in.push_back(InChunk{0, k * span, span});
+        for (uint32_t op = 0; op < 2; ++op)
+            for (uint32_t k = 0; k < count; ++k) in.push_back(InChunk{0, k * span, span, op});
     }
     if (wide_rows(s)) {  // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
         uint32_t first = 0, size = (per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
@@ -632,8 +638,9 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         const uint32_t per_piece = uint32_t(std::max<size_t>(1, kPieceBytes / row));  // rows per piece
         const uint32_t operands = (a_locked ? 0u : 1u) + (b_locked ? 0u : 1u);
         std::vector<uint32_t> first_piece(in.size() + 1, 0);
-        for (uint32_t k = 0; k < in.size(); ++k) {
-            pieces[k] = operands * ((in[k].span + per_piece - 1) / per_piece);
+        for (uint32_t k = 0; k < in.size(); ++k) {  // pageable operands of chunk k x its pieces each
+            const uint32_t ops = in[k].op == InChunk::kBothOperands ? operands : (locked[in[k].op] ? 0u : 1u);
+            pieces[k] = ops * ((in[k].span + per_piece - 1) / per_piece);
             first_piece[k + 1] = first_piece[k] + pieces[k];
             s.packed[k].store(0, std::memory_order_relaxed);
         }
@@ -648,8 +655,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
                  piece = next->fetch_add(1, std::memory_order_relaxed)) {
                 while (piece >= first_piece[k + 1]) ++k;
                 const InChunk ch = in[k];
-                const uint32_t local = piece - first_piece[k], per_op = pieces[k] / operands;
-                const int op = operands == 2 ? int(local / per_op) : (a_locked ? 1 : 0);
+                const uint32_t local = piece - first_piece[k], per_op = (ch.span + per_piece - 1) / per_piece;
+                const int op = ch.op != InChunk::kBothOperands ? int(ch.op)
+                               : operands == 2                 ? int(local / per_op)
+                                                               : (a_locked ? 1 : 0);
                 const size_t first = size_t(local % per_op) * per_piece;
                 const size_t last = std::min<size_t>(ch.span, first + per_piece);
                 if (ordered) {  // gather rows s*j + t to their split-major places t*N' + j
@@ -695,8 +704,10 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
         uint32_t* staged = direct ? s.operands : reinterpret_cast<uint32_t*>(s.dots);
         for (uint32_t k = 0; k < in.size(); ++k) {
             const size_t first = in[k].j0, count = in[k].span, bytes = count * row;  // coefficient range
+            const uint32_t op_first = in[k].op == InChunk::kBothOperands ? 0u : in[k].op;
+            const uint32_t op_count = in[k].op == InChunk::kBothOperands ? 2u : 1u;
             spin_until(s.packed[k], pieces[k], s.team ? s.team->spin_time() : HostTeam::kSpinTime);
-            for (int op = 0; op < 2; ++op) {
+            for (uint32_t op = op_first; op < op_first + op_count; ++op) {
                 const uint32_t* from = src[op] + first * h.limbs;
                 if (!locked[op]) from = s.stage_in + op * words + first * h.limbs;  // packed by the team
                 check(cudaMemcpyAsync(staged + op * words + first * h.limbs, from, bytes, cudaMemcpyHostToDevice,
@@ -707,11 +718,12 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
             check(cudaStreamWaitEvent(st, s.in_ready[k], 0), "cudaStreamWaitEvent");
             if (!direct)
                 launch_pad_rows(staged, s.operands, h.n, h.limbs, s.padded_limbs, split, uint32_t(first),
-                                uint32_t(count), st);
+                                uint32_t(count), st, op_first, op_count);
             // coefficients [first, first + count): j in [first / s, (first + count) / s) of every transform
-            enqueue_convert(s, 0, split, uint32_t(first / split), uint32_t(count / split), st);
+            enqueue_convert(s, 0, split, uint32_t(first / split), uint32_t(count / split), st, op_first, op_count);
+            if (k + 1 == in.size() || in[k + 1].op != in[k].op)  // these operands are complete
+                launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, 0, split, st, op_first, op_count);
         }
-        launch_ntt_forward(s.residues, s.primes, s.fwd, s.r, h.n, n_sub, 0, split, st);
     }
     launch_pointwise(s.residues, s.primes, s.zeta, s.r, h.n, n_sub, split, st);
     launch_ntt_inverse(s.residues, s.primes, s.inv, s.r, h.n, n_sub, 0, split, st);
