@@ -9,6 +9,7 @@
 //  * failures throw std::runtime_error with the library's message.
 // Compile with -DFHERMA_TYPES_DEFINED and the platform's fherma.h included
 // first to use the generated types instead of include/fherma_b200.h's.
+#include <malloc.h>
 #include <sys/mman.h>
 
 #if defined(__x86_64__)
@@ -21,6 +22,7 @@
 
 #include <condition_variable>
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -37,6 +39,8 @@ namespace {
 // its elements on one core, and fresh pages fault one 4 KB page at a time: 156-160 ms for the
 // 458 MB result of N=65536, L=1747 on a B200 host. Reserving first and asking for transparent
 // huge pages over the reserved range (when it spans at least kHugeBytes) cuts that to 54 ms.
+// The hint applies from 4 MB up: behind the reference's harness it also helped the 14.4 MB result
+// of N=65536, L=55 (see keep_heap_resident below for the measurement).
 // After the fill the thread keeps spinning until the call is over (release(), or kActiveFor):
 // on a B200 box's virtual host, copy threads writing lines that this thread had just zeroed,
 // once it slept, took ~300 us for the last 1.8 MB output chunk instead of ~35, and the device's
@@ -75,7 +79,7 @@ public:
     void release() { released_.store(true); }
 
 private:
-    static constexpr size_t kHugeBytes = size_t(32) << 20;
+    static constexpr size_t kHugeBytes = size_t(4) << 20;
     static constexpr std::chrono::milliseconds kActiveFor{50};
 
     static void build(std::vector<uint32_t>& v, size_t count) {
@@ -134,6 +138,22 @@ struct State {
     OutputBuilder output;
 };
 
+// The platform harness allocates the operands and the result of every case afresh and frees them
+// after it. With glibc's defaults the freed heap top goes back to the operating system after each
+// case, so every fherma_run faults the pages of its fresh result vector in again while filling it
+// (one 4 KB page at a time on a virtual host). fherma_init therefore keeps freed heap memory in
+// the process: arrays up to 32 MB come from the heap, and the heap top is trimmed only beyond
+// 1 GB. Behind the reference's harness at N=65536, L=55 this took fherma_run from 1.69 to 1.45 ms
+// together with the huge-page hint above (from 1.69 to 1.52 ms alone), and from 0.532 to 0.518 ms
+// at N=32768, L=28 (medians of 20 cases, 4 alternating runs on one box). Set
+// NEGACYCLIC_KEEP_MALLOC=1 to leave the process's allocator settings alone.
+void keep_heap_resident() {
+    const char* keep = std::getenv("NEGACYCLIC_KEEP_MALLOC");
+    if (keep && *keep && *keep != '0') return;
+    mallopt(M_MMAP_THRESHOLD, 32 << 20);
+    mallopt(M_TRIM_THRESHOLD, 1 << 30);
+}
+
 [[noreturn]] void raise(const char* what) {
     throw std::runtime_error(std::string(what) + ": " + negacyclic_last_error());
 }
@@ -142,6 +162,7 @@ struct State {
 
 void* fherma_init(const fherma::Point& point) {
     if (point.q.data.size() != point.L) throw std::runtime_error("q must hold L words");
+    keep_heap_resident();
     auto* state = new State;
     state->n = point.N;
     state->limbs = point.L;
