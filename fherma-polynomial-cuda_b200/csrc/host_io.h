@@ -25,6 +25,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdint>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -44,6 +45,50 @@
 #endif
 
 namespace negacyclic {
+
+#if defined(__x86_64__) && defined(__GNUC__)
+// dst[0..bytes) = src[0..bytes) with 64-byte streaming (non-temporal) stores from the first
+// 64-byte boundary of dst on: the stores bypass the caches, so filling the page-locked staging
+// does not evict the caller's data and reads nothing of the destination first. The stores are
+// weakly ordered: the caller fences (store_fence) before it publishes the copy to another thread.
+__attribute__((target("avx512f"))) inline void stream_copy_avx512(void* dst, const void* src, size_t bytes) {
+    auto* out = static_cast<unsigned char*>(dst);
+    auto* in = static_cast<const unsigned char*>(src);
+    const size_t head = std::min(bytes, size_t((64 - (reinterpret_cast<uintptr_t>(out) & 63)) & 63));
+    std::memcpy(out, in, head);
+    size_t i = head;
+    for (; i + 256 <= bytes; i += 256) {  // four lines per step: four loads in flight
+        const __m512i v0 = _mm512_loadu_si512(in + i), v1 = _mm512_loadu_si512(in + i + 64);
+        const __m512i v2 = _mm512_loadu_si512(in + i + 128), v3 = _mm512_loadu_si512(in + i + 192);
+        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i), v0);
+        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 64), v1);
+        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 128), v2);
+        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 192), v3);
+    }
+    for (; i + 64 <= bytes; i += 64)
+        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i), _mm512_loadu_si512(in + i));
+    std::memcpy(out + i, in + i, bytes - i);
+}
+#endif
+
+// Copy into page-locked staging: streaming stores where the CPU has AVX-512, memcpy elsewhere.
+inline void stage_copy(void* dst, const void* src, size_t bytes) {
+#if defined(__x86_64__) && defined(__GNUC__)
+    static const bool avx512 = __builtin_cpu_supports("avx512f");
+    if (avx512) {
+        stream_copy_avx512(dst, src, bytes);
+        return;
+    }
+#endif
+    std::memcpy(dst, src, bytes);
+}
+
+// Orders this thread's earlier streaming stores before its later stores (a release publication).
+inline void store_fence() {
+#if defined(__x86_64__) || defined(__i386__)
+    _mm_sfence();
+#endif
+}
 
 class HostTeam {
 public:

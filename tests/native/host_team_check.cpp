@@ -2,7 +2,8 @@
 // run by tests/test_host_team.py: a pack job that publishes per-chunk counters while a launcher
 // thread consumes chunks in order, an unpack job that follows per-chunk "landed" flags, blocking
 // copies and touches, and many calls in a row with idle gaps (with a short spin, workers going to
-// sleep and waking), then that a team whose workers are spinning is destroyed at once.
+// sleep and waking), stage_copy against memcpy, and that a team whose workers are spinning is
+// destroyed at once.
 #include <atomic>
 #include <chrono>
 #include <cstdint>
@@ -95,6 +96,21 @@ int main(int argc, char** argv) {
     {
         HostTeam team(workers, std::chrono::microseconds(200));  // workers sleep in the idle gaps
         run_calls(team, 8);
+    }
+    {  // stage_copy (streaming stores where the CPU has AVX-512): every size and misalignment
+        std::mt19937_64 rng(9);
+        std::vector<unsigned char> src(1 << 16), dst(src.size() + 256);
+        for (auto& x : src) x = static_cast<unsigned char>(rng());
+        for (int trial = 0; trial < 2000; ++trial) {
+            const size_t bytes = trial < 600 ? size_t(trial) : size_t(rng() % (src.size() - 128));
+            const size_t s_off = rng() % 64, d_off = rng() % 128;
+            std::fill(dst.begin(), dst.end(), 0xA5);
+            negacyclic::stage_copy(dst.data() + d_off, src.data() + s_off, bytes);
+            negacyclic::store_fence();
+            EXPECT(std::memcmp(dst.data() + d_off, src.data() + s_off, bytes) == 0);
+            EXPECT(std::all_of(dst.begin(), dst.begin() + d_off, [](unsigned char x) { return x == 0xA5; }));
+            EXPECT(std::all_of(dst.begin() + d_off + bytes, dst.end(), [](unsigned char x) { return x == 0xA5; }));
+        }
     }
     {  // destroying a team whose workers are spinning does not wait out their spin
         auto team = std::make_unique<HostTeam>(workers);
