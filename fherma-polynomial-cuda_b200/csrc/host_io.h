@@ -74,7 +74,7 @@ __attribute__((target("avx512f"))) inline void stream_copy_avx512(void* dst, con
 // Copy into page-locked staging: streaming stores where the CPU has AVX-512, memcpy elsewhere.
 inline void stage_copy(void* dst, const void* src, size_t bytes) {
 #if defined(__x86_64__) && defined(__GNUC__)
-    static const bool avx512 = __builtin_cpu_supports("avx512f");
+    static const bool avx512 = (__builtin_cpu_init(), __builtin_cpu_supports("avx512f"));
     if (avx512) {
         stream_copy_avx512(dst, src, bytes);
         return;
