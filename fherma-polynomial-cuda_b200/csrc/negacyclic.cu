@@ -500,7 +500,8 @@ void ensure_staging(negacyclic_plan& s) {
 // In: rows of at least 1 KB go in transform order: a chunk is part of transform t, positions j
 // in [j0, j0 + span), i.e. coefficients s*j + t (one 2-D copy per operand), so the forward NTTs
 // of transform t run while later transforms are still being copied in. Narrower rows go as
-// contiguous coefficient ranges, whose forward NTTs wait for the last chunk.
+// contiguous coefficient ranges of operand a, then of operand b, so that a's forward NTTs run
+// while b is still being copied in.
 // Out: contiguous coefficient ranges; each chunk's copy-out overlaps the next chunk's CRT GEMM
 // and reduction.
 struct InChunk {  // transform t, positions j in [j0, j0 + span): coefficients s*j + t
@@ -527,9 +528,11 @@ uint32_t chunk_count(size_t bytes, size_t target, uint32_t most, uint32_t limit)
 
 // Chunk lists of a streamed host product (at most kMaxChunks each way).
 // In, transform-ordered: `parts` chunks per transform, the last transform cut finer, so that
-// little conversion is left once the link has delivered everything. In, coefficient-ordered:
-// equal coefficient ranges, the last one cut in four. Out: coefficient ranges growing from a
-// quarter of a chunk, so the copy-out starts soon after the last inverse NTT.
+// little conversion is left once the link has delivered everything. In, coefficient-ordered,
+// wide rows: equal coefficient ranges of both operands, the last one cut in four; narrow rows:
+// equal ranges of operand a, then of operand b. Out, wide rows: coefficient ranges growing from
+// a quarter of a chunk, so the copy-out starts soon after the last inverse NTT; narrow rows:
+// equal ranges of about 1 MB.
 void stream_chunks(const negacyclic_plan& s, bool ordered, std::vector<InChunk>& in, std::vector<OutChunk>& out) {
     const HostPlan& h = s.host;
     const uint32_t split = h.split, n_sub = h.n_sub, per = h.n / s.chunks;
