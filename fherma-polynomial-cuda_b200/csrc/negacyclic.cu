@@ -289,9 +289,7 @@ int negacyclic_init(uint32_t n, uint32_t w, uint32_t limbs, const uint32_t* q, c
         check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&s.copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaStreamCreateWithFlags(&s.copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
-        // host products stream in transform-ordered chunks (max(8, s) of them) once each chunk
-        // keeps 128-row GEMM tiles
-        s.chunks = (h.n_sub >= 1024 && h.n >= 8192) ? std::max(8u, h.split) : 1;
+        s.chunks = host_chunks(h.n, h.n_sub, h.split);  // csrc/host_chunks.h
         for (uint32_t c = 0; c < (s.chunks > 1 ? negacyclic_plan::kMaxChunks : 1u); ++c) {
             check(cudaEventCreateWithFlags(&s.in_ready[c], cudaEventDisableTiming), "cudaEventCreate");
             check(cudaEventCreateWithFlags(&s.out_ready[c], cudaEventDisableTiming), "cudaEventCreate");
@@ -496,104 +494,9 @@ void ensure_staging(negacyclic_plan& s) {
     }
 }
 
-// Streamed host products run in about max(8, s) chunks each way (stream_chunks below).
-// In: rows of at least 1 KB go in transform order: a chunk is part of transform t, positions j
-// in [j0, j0 + span), i.e. coefficients s*j + t (one 2-D copy per operand), so the forward NTTs
-// of transform t run while later transforms are still being copied in. Narrower rows go as
-// contiguous coefficient ranges of operand a, then of operand b, so that a's forward NTTs run
-// while b is still being copied in.
-// Out: contiguous coefficient ranges; each chunk's copy-out overlaps the next chunk's CRT GEMM
-// and reduction.
-struct InChunk {  // transform t, positions j in [j0, j0 + span): coefficients s*j + t
-    uint32_t t, j0, span;
-    uint32_t op = kBothOperands;  // operand 0 (a) or 1 (b), or both
-    static constexpr uint32_t kBothOperands = 2;
-};
-struct OutChunk {  // coefficients [first, first + count)
-    uint32_t first, count;
-};
-
-bool transform_ordered_input(const negacyclic_plan& s, bool packed_by_team);
-
-// Rows of at least 1 KB: chunks carry enough work that finer chunks near the ends (and one
-// transpose per output chunk) pay for their extra launches. Narrower rows keep equal chunks.
-bool wide_rows(const negacyclic_plan& s) { return s.host.limbs >= 256; }
-
-// Chunks of about `target` bytes out of `bytes`: a power of two in [2, min(most, limit)].
-uint32_t chunk_count(size_t bytes, size_t target, uint32_t most, uint32_t limit) {
-    uint32_t count = 2;
-    while (count * 2 <= std::min(most, limit) && bytes / (count * 2) >= target) count *= 2;
-    return std::max(1u, std::min(count, std::min(most, limit)));
-}
-
-// Chunk lists of a streamed host product (at most kMaxChunks each way).
-// In, transform-ordered: `parts` chunks per transform, the last transform cut finer, so that
-// little conversion is left once the link has delivered everything. In, coefficient-ordered,
-// wide rows: equal coefficient ranges of both operands, the last one cut in four; narrow rows:
-// equal ranges of operand a, then of operand b. Out, wide rows: coefficient ranges growing from
-// a quarter of a chunk, so the copy-out starts soon after the last inverse NTT; narrow rows:
-// equal ranges of about 1 MB.
-void stream_chunks(const negacyclic_plan& s, bool ordered, std::vector<InChunk>& in, std::vector<OutChunk>& out) {
-    const HostPlan& h = s.host;
-    const uint32_t split = h.split, n_sub = h.n_sub, per = h.n / s.chunks;
-    constexpr uint32_t kMax = negacyclic_plan::kMaxChunks;
-    in.clear();
-    out.clear();
-    if (s.chunks == 1) {  // small product: one piece each way
-        in.push_back(InChunk{0, 0, h.n});
-        out.push_back(OutChunk{0, h.n});
-        return;
-    }
-    if (ordered) {
-        const uint32_t parts = s.chunks / split;
-        uint32_t tail = parts;  // power of two, spans of >= 256 rows, within the event budget
-        while (tail * 2 <= 4 * parts && (split - 1) * parts + tail * 2 <= kMax && n_sub / (tail * 2) >= 256) tail *= 2;
-        for (uint32_t t = 0; t < split; ++t) {
-            const uint32_t p = t + 1 == split ? tail : parts, span = n_sub / p;
-            for (uint32_t k = 0; k < p; ++k) in.push_back(InChunk{t, k * span, span});
-        }
-    } else if (wide_rows(s)) {
-        const uint32_t quarter = per / 4;
-        const bool cut = quarter / split >= 256 && s.chunks + 3 <= kMax;
-        for (uint32_t k = 0; k + 1 < s.chunks; ++k) in.push_back(InChunk{0, k * per, per});
-        if (cut)
-            for (uint32_t k = 0; k < 4; ++k) in.push_back(InChunk{0, (s.chunks - 1) * per + k * quarter, quarter});
-        else
-            in.push_back(InChunk{0, (s.chunks - 1) * per, per});
-    } else {
-        // narrow rows: operand a, then operand b, each in coefficient ranges of about 1 MB (at
-        // least two per operand, and at least 256 positions of every transform each), so that a's
-        // conversion and forward NTTs run while b is still on the way. Small copies carry fixed
-        // costs: 0.46 MB host-to-device copies ran at 23 GB/s against 55 for large ones (N=32768,
-        // L=28).
-        const uint32_t count = chunk_count(size_t(h.n) * h.limbs * 4, 1u << 20, std::min(s.chunks, kMax / 2),
-                                           n_sub / 256);
-        const uint32_t span = h.n / count;
-        for (uint32_t op = 0; op < 2; ++op)
-            for (uint32_t k = 0; k < count; ++k) in.push_back(InChunk{0, k * span, span, op});
-    }
-    if (wide_rows(s)) {  // per/4, per/4, per/2, then whole chunks: two chunks more than the plain split
-        uint32_t first = 0, size = (per / 4 >= 256 && s.chunks + 2 <= kMax) ? per / 4 : per;
-        for (uint32_t k = 0; first < h.n; ++k) {
-            const uint32_t count = std::min(size, h.n - first);
-            out.push_back(OutChunk{first, count});
-            first += count;
-            if (k >= 1 && size < per) size *= 2;  // per/4, per/4, per/2, per, per, ...
-        }
-        return;
-    }
-    // narrow rows: about 1 MB of result per chunk, at least 256 coefficients each
-    const uint32_t count = chunk_count(size_t(h.n) * h.limbs * 4, 1u << 20, s.chunks, h.n / 256);
-    for (uint32_t k = 0; k < count; ++k) out.push_back(OutChunk{k * (h.n / count), h.n / count});
-}
-
-// Transform order needs rows gathered with a stride of s rows, by the copy engine as a 2-D copy
-// or by the host team while it packs pageable operands. Both pay only for rows of 1 KB or more:
-// a 2-D copy of 220-byte rows ran at a third of the link rate, and the team gathering 220-byte
-// rows packed at 20 GB/s against 55 GB/s for contiguous ranges (N=65536, L=55).
-bool transform_ordered_input(const negacyclic_plan& s, bool packed_by_team) {
-    (void)packed_by_team;
-    return s.chunks > 1 && s.host.split > 1 && wide_rows(s);  // chunks >= split when chunked
+// The plan's shape for the chunk lists (csrc/host_chunks.h).
+ChunkShape chunk_shape(const negacyclic_plan& s) {
+    return ChunkShape{s.host.n, s.host.n_sub, s.host.split, s.host.limbs, s.chunks};
 }
 
 void copy_rows_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row, uint32_t rows,
@@ -629,8 +532,8 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     // every chunk is converted, stages them
     std::vector<InChunk> in;
     std::vector<OutChunk> out;
-    const bool ordered = transform_ordered_input(s, !a_locked && !b_locked);
-    stream_chunks(s, ordered, in, out);
+    const bool ordered = transform_ordered_input(chunk_shape(s));
+    stream_chunks(chunk_shape(s), ordered, in, out);
     uint32_t pieces[negacyclic_plan::kMaxChunks] = {};  // pack pieces per input chunk
     if (!a_locked || !b_locked) {
         // One pack job over pieces of about kPieceBytes of the pageable operands, claimed in chunk
@@ -739,7 +642,7 @@ void host_begin(negacyclic_plan& s, const uint32_t* a, const uint32_t* b, uint32
     // chunk's work. With wide rows the transpose also goes chunk by chunk, so only the first
     // chunk's share sits between the inverse NTT and the first copy-out.
     uint32_t* dst = s.outputs_staged ? s.stage_out : c;
-    const bool transpose_per_chunk = wide_rows(s);
+    const bool transpose_per_chunk = wide_rows(chunk_shape(s));
     if (!transpose_per_chunk) launch_transpose(s.residues, s.crt_in, s.r, s.padded_r, h.n, split, 0, n_sub, st);
     for (uint32_t k = 0; k <= out.size(); ++k) {
         if (k < out.size()) {
@@ -774,7 +677,7 @@ int host_finish(negacyclic_plan& s, uint32_t* c) {
     if (s.outputs_staged) {
         std::vector<InChunk> in;
         std::vector<OutChunk> out;
-        stream_chunks(s, false, in, out);  // the output chunks do not depend on the input order
+        stream_chunks(chunk_shape(s), false, in, out);  // the output chunks do not depend on the input order
         // one unpack job per output chunk, posted as soon as its copy-out has completed: the
         // workers copy their slices of it into c while later chunks are still on the way (and
         // sleep, instead of spinning, while the device computes)

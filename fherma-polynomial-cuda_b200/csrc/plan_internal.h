@@ -8,6 +8,7 @@
 #include "../../include/negacyclic.h"
 #include "gemm_tc.cuh"
 #include "host_plan.h"
+#include "host_chunks.h"
 #include "host_io.h"
 #include "kernels.cuh"
 
@@ -36,7 +37,7 @@ struct negacyclic_plan {
     size_t work_bytes = 0;
     bool gemm_tensor_wanted = true, gemm_tensor_required = false, gemm_pairs_allowed = true;
     cudaStream_t stream = nullptr, copy_in = nullptr, copy_out = nullptr;
-    static constexpr uint32_t kMaxChunks = 16;
+    static constexpr uint32_t kMaxChunks = negacyclic::kMaxHostChunks;
     uint32_t chunks = 1;  // coefficient chunks of the streamed host path
     cudaEvent_t in_ready[kMaxChunks] = {};
     cudaEvent_t out_ready[kMaxChunks] = {};
