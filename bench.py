@@ -68,7 +68,11 @@ CPU_FULL_OVER_SAMPLE = 19.35  # 77.74 s against 4.01 s (median of 3), 16-core Xe
 # capture (dram__bytes_read.sum 4.32 GB + dram__bytes_write.sum 1.90 GB) of
 #   python bench.py --workload 65536,1747 --steps 1 --warmup 1 --device-only
 CONVERT_DRAM_BYTES = 6.22e9
-CONVERT_TENSOR_PIPE_ACTIVE = 0.833
+# sm__pipe_tensor_cycles_active of the conversion GEMM alone, from the single-kernel capture
+#   ncu --set full --clock-control none -k regex:gemm_tc -c 2 \
+#       python bench.py --workload 16384,1747 --steps 1 --warmup 1 --device-only
+# (profiles/gemm_tc_N16384_L1747.md): the clock-free fraction of the int8 tensor pipe's peak
+CONVERT_TENSOR_PIPE_ACTIVE = 0.836
 
 
 def _load(name, path, package_dir=None):
