@@ -47,27 +47,35 @@
 namespace negacyclic {
 
 #if defined(__x86_64__) && defined(__GNUC__)
-// dst[0..bytes) = src[0..bytes) with 64-byte streaming (non-temporal) stores from the first
-// 64-byte boundary of dst on: the stores bypass the caches, so filling the page-locked staging
-// does not evict the caller's data and reads nothing of the destination first. The stores are
-// weakly ordered: the caller fences (store_fence) before it publishes the copy to another thread.
+// dst[0..bytes) = src[0..bytes), writing every whole 64-byte line of the destination with a
+// streaming (non-temporal) store and the partial lines at either end with memcpy. Streaming stores
+// bypass the caches, so filling the page-locked staging neither evicts the caller's data nor reads
+// the destination first. They are weakly ordered: the caller fences (store_fence) before it
+// publishes the copy to another thread.
 __attribute__((target("avx512f"))) inline void stream_copy_avx512(void* dst, const void* src, size_t bytes) {
-    auto* out = static_cast<unsigned char*>(dst);
-    auto* in = static_cast<const unsigned char*>(src);
-    const size_t head = std::min(bytes, size_t((64 - (reinterpret_cast<uintptr_t>(out) & 63)) & 63));
-    std::memcpy(out, in, head);
-    size_t i = head;
-    for (; i + 256 <= bytes; i += 256) {  // four lines per step: four loads in flight
-        const __m512i v0 = _mm512_loadu_si512(in + i), v1 = _mm512_loadu_si512(in + i + 64);
-        const __m512i v2 = _mm512_loadu_si512(in + i + 128), v3 = _mm512_loadu_si512(in + i + 192);
-        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i), v0);
-        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 64), v1);
-        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 128), v2);
-        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i + 192), v3);
+    char* const out = static_cast<char*>(dst);
+    const char* const in = static_cast<const char*>(src);
+    const uintptr_t start = reinterpret_cast<uintptr_t>(out), stop = start + bytes;
+    const uintptr_t lines_from = (start + 63) & ~uintptr_t(63), lines_to = stop & ~uintptr_t(63);
+    if (lines_to <= lines_from) {  // no whole line inside the destination
+        std::memcpy(out, in, bytes);
+        return;
     }
-    for (; i + 64 <= bytes; i += 64)
-        _mm512_stream_si512(reinterpret_cast<__m512i*>(out + i), _mm512_loadu_si512(in + i));
-    std::memcpy(out + i, in + i, bytes - i);
+    const size_t lead = lines_from - start, lines = (lines_to - lines_from) / 64;
+    std::memcpy(out, in, lead);
+    __m512i* line = reinterpret_cast<__m512i*>(out + lead);
+    const char* from = in + lead;
+    size_t k = 0;
+    for (; k + 2 <= lines; k += 2, from += 128) {  // two lines per step
+        const __m512i first = _mm512_loadu_si512(from), second = _mm512_loadu_si512(from + 64);
+        _mm512_stream_si512(line + k, first);
+        _mm512_stream_si512(line + k + 1, second);
+    }
+    if (k < lines) {
+        _mm512_stream_si512(line + k, _mm512_loadu_si512(from));
+        from += 64;
+    }
+    std::memcpy(out + (lines_to - start), from, stop - lines_to);
 }
 #endif
 
